@@ -1,0 +1,169 @@
+/*
+ * rssieve_b200.h -- C ABI of the B200 RSSieve sieve library.
+ *
+ * The reference (mfl0p/RSSieve) has no plugin or FFI API: it is a process
+ * (main.cpp) whose hot path lives in cl_sieve.cpp + simpleCL.c and a set of
+ * OpenCL kernels.  This header is the seam that replaces that internal layer:
+ * plain C types, caller-owned host buffers, library-owned device memory, one
+ * CUDA device per context, every entry point returns an error code (never
+ * exits).  A context is not reentrant; use one per host thread.
+ *
+ * Terms are k*b^n + c with c = +1 or -1; "seq" indexes the sequences of a job.
+ * k is 64-bit here (the reference stores it as int, inputfile.cpp:366).
+ */
+#ifndef RSSIEVE_B200_H
+#define RSSIEVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RS_MAX_SEQ 100          /* MAX_SEQUENCES, cl_sieve.h:2 */
+
+/* error codes */
+#define RS_OK 0
+#define RS_EARG (-1)            /* invalid argument or state */
+#define RS_ECUDA (-2)           /* CUDA runtime error (message in rs_last_error) */
+#define RS_ENOMEM (-3)
+#define RS_EDEVICE (-4)         /* a kernel raised an internal error flag */
+#define RS_EIO (-5)             /* file open/read/write failure */
+#define RS_EPARSE (-6)          /* malformed input file */
+#define RS_ESTATE (-7)          /* checkpoint missing, corrupt or for another job */
+#define RS_EVERIFY (-8)         /* a device factor failed host verification */
+#define RS_ENODEV (-9)          /* no CUDA device / library built without one */
+
+/* One job: up to 100 sequences sharing a base and an n-range.  Mirrors the
+ * job fields of workStatus (cl_sieve.h:21-26) plus the candidate bitmap of
+ * searchData (cl_sieve.h:30-36, inputfile.cpp:15-21): word seq*words_per_seq
+ * + (n-nmin)/32, bit (n-nmin)%32, 1 = term still a candidate. */
+typedef struct rs_seqs {
+    uint32_t base;
+    uint32_t kcount;
+    uint32_t nmin;
+    uint32_t nmax;
+    uint64_t k[RS_MAX_SEQ];
+    int32_t c[RS_MAX_SEQ];
+    uint64_t words_per_seq;
+    uint32_t *bitmap;           /* owned by the rs_seqs object */
+} rs_seqs;
+
+/* A found factor p | k[seq]*b^n + c[seq]; replaces struct factor (cl_sieve.h:4-8),
+ * which carried the signed int k instead of the sequence index. */
+typedef struct rs_factor {
+    uint64_t p;
+    uint32_t n;
+    uint32_t seq;
+} rs_factor;
+
+/* Device counters.  primes = primes tested (the reference's g_sum/primecount,
+ * setup.cl:99-101, which counts 2-PRPs); dups = solutions whose term was
+ * already eliminated or is not a candidate (g_primecount[6], giant.cl:195-196,
+ * counted here for n in [nmin,nmax] only). */
+typedef struct rs_counters {
+    uint64_t primes;
+    uint64_t skipped;           /* p | b, p | some k, or no solvable k */
+    uint64_t full;              /* primes searched over every n */
+    uint64_t parity;            /* primes searched over one parity of n */
+    uint64_t targets;           /* sum of surviving k over searched primes */
+    uint64_t baby;              /* baby steps */
+    uint64_t giant;             /* giant steps = Montgomery products + probes */
+    uint64_t small_order;       /* primes where ord(b^e) < Q */
+    uint64_t candidates;        /* fingerprint matches verified */
+    uint64_t hits;              /* verified solutions with n in [nmin,nmax] (factors + dups) */
+    uint64_t factors;           /* terms eliminated */
+    uint64_t dups;
+    uint64_t sieve_cands;       /* reserved */
+} rs_counters;
+
+/* checkpoint scalars of workStatus (cl_sieve.h:21-26) */
+typedef struct rs_state {
+    uint64_t pmin, pmax, p, checksum, primecount, factorcount, last_trickle, dupcount;
+} rs_state;
+
+/* ---------------- host services (no GPU needed) ---------------- */
+
+const char *rs_version(void);
+const char *rs_strerror(int code);
+/* detail of the last error on the calling thread */
+const char *rs_last_error(void);
+
+/* ABCD input (sr2sieve/sr5sieve format); replaces read_input, inputfile.cpp:251-465.
+ * Same rules: one base, c = +-1, <= 100 sequences, k > 0, n0 > 0, delta lines,
+ * '#' comments; nmin is rounded down to even.  k may be up to 2^64-1. */
+int rs_abcd_parse(const char *text, size_t len, rs_seqs **out);
+int rs_abcd_read(const char *path, rs_seqs **out);
+/* Build a job directly; bitmap may be NULL (all n in [nmin,nmax] are candidates). */
+int rs_seqs_create(uint32_t base, uint32_t kcount, const uint64_t *k, const int32_t *c, uint32_t nmin,
+                   uint32_t nmax, const uint32_t *bitmap, rs_seqs **out);
+void rs_seqs_free(rs_seqs *s);
+/* number of candidate terms (set bits) */
+uint64_t rs_seqs_count(const rs_seqs *s);
+
+/* verify_factor.c:131-181: 1 if p is prime and p | k*b^n+c, 0 if not a factor,
+ * -1 if p is composite. */
+int rs_verify_factor(uint64_t p, uint64_t k, uint32_t n, int32_t c, uint32_t base);
+/* deterministic primality below 2^64 (verify_factor.c:100-128) */
+int rs_is_prime(uint64_t n);
+
+/* "p | k*b^n+c\n" exactly as cl_sieve.cpp:624 prints it */
+int rs_format_factor(const rs_seqs *s, const rs_factor *f, char *buf, size_t len);
+/* read_factors_file_update_bitmap, cl_sieve.cpp:797-863: clear the bitmap bit
+ * of every term listed in a factor file; *lines = number of lines read. */
+int rs_factors_file_apply(const char *path, rs_seqs *s, uint64_t *lines);
+/* getResults' host half, cl_sieve.cpp:590-631: sort by (p,n), verify each
+ * factor, drop composite p, append the lines to path, update state checksum
+ * and factorcount.  Returns RS_EVERIFY (and writes nothing) on a false factor. */
+int rs_factors_commit(const char *path, const rs_seqs *s, rs_factor *f, size_t n, rs_state *st);
+/* finalizeResults, cl_sieve.cpp:738-795 */
+int rs_factors_finalize(const char *path, const rs_state *st);
+
+/* Checkpoint files; replace write_state/read_state, cl_sieve.cpp:185-319.
+ * When every k < 2^31 the file is the reference's 488-byte workStatus layout
+ * with its additive state_sum; otherwise a versioned layout with 64-bit k.
+ * rs_state_read validates the checksum and the job fields and fails with
+ * RS_ESTATE otherwise. */
+int rs_state_write(const char *path, const rs_state *st, const rs_seqs *s);
+int rs_state_read(const char *path, rs_state *st, const rs_seqs *s);
+/* Both A/B files: newest valid one wins (cl_sieve.cpp:288-318).  Returns 1 and
+ * fills st and which (0 = A, 1 = B) when a valid state exists, 0 when none. */
+int rs_state_resume(const char *path_a, const char *path_b, rs_state *st, const rs_seqs *s, int *which);
+
+/* ---------------- device ---------------- */
+
+typedef struct rs_ctx rs_ctx;
+
+/* Context on one CUDA device (replaces sclHard/progData, cl_sieve.h:39-49 and
+ * the device set-up of main.cpp:260-303). */
+int rs_ctx_create(int device, rs_ctx **out);
+void rs_ctx_destroy(rs_ctx *ctx);
+/* Launch on a caller stream (cudaStream_t as void*); NULL = the context's own. */
+int rs_ctx_set_stream(rs_ctx *ctx, void *stream);
+int rs_device_count(void);
+
+/* Upload a job: sequences, n-range and bitmap (cl_sieve.cpp:1115-1120,1266). */
+int rs_job_load(rs_ctx *ctx, const rs_seqs *s);
+/* Sieve every prime in [p0,p1) (3 <= p0 < p1 <= 2^64-1): one pass of the
+ * segment loop cl_sieve.cpp:1292-1403.  Found factors accumulate on the
+ * device; *delta (may be NULL) receives this call's counters. */
+int rs_run_range(rs_ctx *ctx, uint64_t p0, uint64_t p1, rs_counters *delta);
+/* Copy out and clear the accumulated factors (the device half of getResults,
+ * cl_sieve.cpp:537-590).  With cap too small, returns RS_EARG and *n = count. */
+int rs_factors_fetch(rs_ctx *ctx, rs_factor *buf, size_t cap, size_t *n);
+/* Download the device bitmap (for checkpoints and tests). */
+int rs_bitmap_download(rs_ctx *ctx, uint32_t *dst, size_t words);
+/* cumulative counters since rs_job_load */
+int rs_counters_get(rs_ctx *ctx, rs_counters *out);
+/* The prime generator alone: odd primes in [p0,p1), unordered, for tests. */
+int rs_primes_generate(rs_ctx *ctx, uint64_t p0, uint64_t p1, uint64_t *dst, size_t cap, size_t *n);
+/* average duration (ms) of the BSGS kernel launches of the last rs_run_range,
+ * measured with CUDA events on the launching stream, and the launch count */
+int rs_last_timing(rs_ctx *ctx, double *bsgs_ms, double *total_kernel_ms, uint32_t *bsgs_launches,
+                   uint32_t *kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

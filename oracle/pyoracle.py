@@ -97,6 +97,8 @@ def ref():
         R.rsref_verify_factor.argtypes = [u64, u64, u32, i32, u32]
         R.rsref_is_prime.restype = C.c_int
         R.rsref_is_prime.argtypes = [u64]
+        R.rsref_sprp2.restype = C.c_int
+        R.rsref_sprp2.argtypes = [u64]
         _ref = R
     return _ref
 
@@ -226,6 +228,14 @@ def ref_verify_factor(p, k, n, c, base):
 
 def ref_is_prime(p):
     return bool(ref().rsref_is_prime(p))
+
+
+def ref_sprp2(n):
+    return bool(ref().rsref_sprp2(n))
+
+
+def sprp2(n):
+    return bool(lib().or_sprp2(n))
 
 
 def verify_and_sort(job, factors):

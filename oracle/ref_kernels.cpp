@@ -198,7 +198,20 @@ int rsref_is_prime(uint64_t p)
     return refv::isPrime(p, q, one, pmo, two, t) ? 1 : 0;
 }
 
-/* strong_prp_two of getsegprimes.cl is not C++; its helpers in common.cl are */
+/* strong_prp_two of getsegprimes.cl is not C++; the same base-2 strong PRP
+ * test is verify_factor.c's strong_prp (verify_factor.c:57-95) with base 2 */
+int rsref_sprp2(uint64_t n)
+{
+    if (n < 3 || !(n & 1)) return 0;
+    uint64_t q = refv::invert(n), one = (0 - n) % n, pmo = n - one, two = refv::add(one, one, n);
+    uint64_t t = refv::add(two, two, n);
+    for (int i = 0; i < 5; ++i) t = refv::m_mul(t, t, n, q);
+    int tz = __builtin_ctzll(n - 1);
+    uint64_t exp = n >> tz;
+    uint64_t cur = 0x8000000000000000ULL >> ((__builtin_clzll(exp) + 1) & 63);
+    return refv::strong_prp(2, n, q, one, pmo, t, tz, exp, cur) ? 1 : 0;
+}
+
 uint64_t rsref_m_mul(uint64_t a, uint64_t b, uint64_t p, uint64_t q) { return ref_b2::m_mul(a, b, p, q); }
 uint64_t rsref_invert(uint64_t p) { return ref_b2::invert(p); }
 uint64_t rsref_powmodlg(uint64_t mbase, uint64_t exp, uint64_t p, uint64_t q) { return ref_b2::powmodlg(mbase, exp, p, q); }

@@ -1,0 +1,322 @@
+"""rssieve_b200 -- B200 (sm_100a) implementation of RSSieve's BSGS sieve path.
+
+Python binding of the C ABI in include/rssieve_b200.h (librssieve_b200.so,
+built in-tree by rssieve_b200.build).  The product is the shared library and
+the `rssieve` command-line drop-in next to it; this module is the host-side
+mirror used by tests and bench.py.  There is no CPU fallback: device entry
+points raise RuntimeError when the library or a CUDA device is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "_lib", "librssieve_b200.so")
+CLI_PATH = os.path.join(PKG, "_lib", "rssieve")
+MAX_SEQ = 100
+
+RS_OK, RS_EARG, RS_ECUDA, RS_ENOMEM, RS_EDEVICE, RS_EIO, RS_EPARSE, RS_ESTATE, RS_EVERIFY, RS_ENODEV = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
+
+FACTOR_DT = np.dtype([("p", "<u8"), ("n", "<u4"), ("seq", "<u4")])
+COUNTER_FIELDS = ("primes", "skipped", "full", "parity", "targets", "baby", "giant", "small_order",
+                  "candidates", "hits", "factors", "dups", "sieve_cands")
+
+
+class _Seqs(C.Structure):
+    _fields_ = [("base", C.c_uint32), ("kcount", C.c_uint32), ("nmin", C.c_uint32), ("nmax", C.c_uint32),
+                ("k", C.c_uint64 * MAX_SEQ), ("c", C.c_int32 * MAX_SEQ), ("words_per_seq", C.c_uint64),
+                ("bitmap", C.POINTER(C.c_uint32))]
+
+
+class _Counters(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in COUNTER_FIELDS]
+
+
+class _State(C.Structure):
+    _fields_ = [(f, C.c_uint64) for f in ("pmin", "pmax", "p", "checksum", "primecount", "factorcount",
+                                          "last_trickle", "dupcount")]
+
+
+class _Factor(C.Structure):
+    _fields_ = [("p", C.c_uint64), ("n", C.c_uint32), ("seq", C.c_uint32)]
+
+
+# every symbol include/rssieve_b200.h declares
+EXPORTS = (
+    "rs_version", "rs_strerror", "rs_last_error", "rs_abcd_parse", "rs_abcd_read", "rs_seqs_create",
+    "rs_seqs_free", "rs_seqs_count", "rs_verify_factor", "rs_is_prime", "rs_format_factor",
+    "rs_factors_file_apply", "rs_factors_commit", "rs_factors_finalize", "rs_state_write", "rs_state_read",
+    "rs_state_resume", "rs_ctx_create", "rs_ctx_destroy", "rs_ctx_set_stream", "rs_device_count",
+    "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
+    "rs_primes_generate", "rs_last_timing",
+)
+
+_lib = None
+
+
+def lib():
+    """Load librssieve_b200.so (building it first when absent and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build
+        build.build()
+    L = C.CDLL(LIB_PATH)
+    u64, u32, i32, vp, sz = C.c_uint64, C.c_uint32, C.c_int32, C.c_void_p, C.c_size_t
+    PS = C.POINTER(_Seqs)
+    sig = {
+        "rs_version": (C.c_char_p, []),
+        "rs_strerror": (C.c_char_p, [C.c_int]),
+        "rs_last_error": (C.c_char_p, []),
+        "rs_abcd_parse": (C.c_int, [C.c_char_p, sz, C.POINTER(PS)]),
+        "rs_abcd_read": (C.c_int, [C.c_char_p, C.POINTER(PS)]),
+        "rs_seqs_create": (C.c_int, [u32, u32, vp, vp, u32, u32, vp, C.POINTER(PS)]),
+        "rs_seqs_free": (None, [PS]),
+        "rs_seqs_count": (u64, [PS]),
+        "rs_verify_factor": (C.c_int, [u64, u64, u32, i32, u32]),
+        "rs_is_prime": (C.c_int, [u64]),
+        "rs_format_factor": (C.c_int, [PS, C.POINTER(_Factor), C.c_char_p, sz]),
+        "rs_factors_file_apply": (C.c_int, [C.c_char_p, PS, C.POINTER(u64)]),
+        "rs_factors_commit": (C.c_int, [C.c_char_p, PS, vp, sz, C.POINTER(_State)]),
+        "rs_factors_finalize": (C.c_int, [C.c_char_p, C.POINTER(_State)]),
+        "rs_state_write": (C.c_int, [C.c_char_p, C.POINTER(_State), PS]),
+        "rs_state_read": (C.c_int, [C.c_char_p, C.POINTER(_State), PS]),
+        "rs_state_resume": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_State), PS, C.POINTER(C.c_int)]),
+        "rs_ctx_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+        "rs_ctx_destroy": (None, [vp]),
+        "rs_ctx_set_stream": (C.c_int, [vp, vp]),
+        "rs_device_count": (C.c_int, []),
+        "rs_job_load": (C.c_int, [vp, PS]),
+        "rs_run_range": (C.c_int, [vp, u64, u64, C.POINTER(_Counters)]),
+        "rs_factors_fetch": (C.c_int, [vp, vp, sz, C.POINTER(sz)]),
+        "rs_bitmap_download": (C.c_int, [vp, vp, sz]),
+        "rs_counters_get": (C.c_int, [vp, C.POINTER(_Counters)]),
+        "rs_primes_generate": (C.c_int, [vp, u64, u64, vp, sz, C.POINTER(sz)]),
+        "rs_last_timing": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(u32),
+                                     C.POINTER(u32)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype, f.argtypes = res, args
+    _lib = L
+    return L
+
+
+class RSError(RuntimeError):
+    def __init__(self, code, what=""):
+        L = lib()
+        msg = "%s: %s (%s)" % (what, L.rs_strerror(code).decode(), L.rs_last_error().decode())
+        super().__init__(msg)
+        self.code = code
+
+
+def _check(rc, what):
+    if rc != RS_OK:
+        raise RSError(rc, what)
+
+
+class Seqs:
+    """A job: up to 100 sequences k*b^n+c over [nmin,nmax] with a candidate bitmap (rs_seqs)."""
+
+    def __init__(self, ptr):
+        self._p = ptr
+
+    @classmethod
+    def from_abcd_text(cls, text):
+        L = lib()
+        p = C.POINTER(_Seqs)()
+        data = text.encode() if isinstance(text, str) else text
+        _check(L.rs_abcd_parse(data, len(data), C.byref(p)), "rs_abcd_parse")
+        return cls(p)
+
+    @classmethod
+    def from_abcd_file(cls, path):
+        L = lib()
+        p = C.POINTER(_Seqs)()
+        _check(L.rs_abcd_read(os.fsencode(path), C.byref(p)), "rs_abcd_read")
+        return cls(p)
+
+    @classmethod
+    def create(cls, base, ks, cs, nmin, nmax, bitmap=None):
+        L = lib()
+        ks = np.ascontiguousarray(ks, dtype=np.uint64)
+        cs = np.ascontiguousarray(cs, dtype=np.int32)
+        bm = None if bitmap is None else np.ascontiguousarray(bitmap, dtype=np.uint32)
+        p = C.POINTER(_Seqs)()
+        _check(L.rs_seqs_create(base, len(ks), ks.ctypes.data, cs.ctypes.data, nmin, nmax,
+                                None if bm is None else bm.ctypes.data, C.byref(p)), "rs_seqs_create")
+        return cls(p)
+
+    def __del__(self):
+        if getattr(self, "_p", None) and _lib is not None:
+            _lib.rs_seqs_free(self._p)
+            self._p = None
+
+    @property
+    def s(self):
+        return self._p.contents
+
+    base = property(lambda self: self.s.base)
+    kcount = property(lambda self: self.s.kcount)
+    nmin = property(lambda self: self.s.nmin)
+    nmax = property(lambda self: self.s.nmax)
+    words_per_seq = property(lambda self: self.s.words_per_seq)
+
+    @property
+    def k(self):
+        return [int(self.s.k[i]) for i in range(self.kcount)]
+
+    @property
+    def c(self):
+        return [int(self.s.c[i]) for i in range(self.kcount)]
+
+    @property
+    def bitmap(self):
+        """numpy view [kcount, words_per_seq] of the library-owned bitmap."""
+        n = self.kcount * self.words_per_seq
+        arr = np.ctypeslib.as_array(self.s.bitmap, shape=(n,))
+        return arr.reshape(self.kcount, self.words_per_seq)
+
+    def count(self):
+        return int(lib().rs_seqs_count(self._p))
+
+    def format_factor(self, p, n, seq):
+        f = _Factor(p, n, seq)
+        buf = C.create_string_buffer(160)
+        _check(lib().rs_format_factor(self._p, C.byref(f), buf, 160), "rs_format_factor")
+        return buf.value.decode()
+
+    def apply_factor_file(self, path):
+        lines = C.c_uint64(0)
+        _check(lib().rs_factors_file_apply(os.fsencode(path), self._p, C.byref(lines)), "rs_factors_file_apply")
+        return int(lines.value)
+
+
+class State:
+    """Checkpoint scalars (workStatus)."""
+
+    def __init__(self, **kw):
+        self.st = _State(**kw)
+
+    def __getattr__(self, k):
+        return getattr(self.__dict__["st"], k)
+
+    def write(self, path, seqs):
+        _check(lib().rs_state_write(os.fsencode(path), C.byref(self.st), seqs._p), "rs_state_write")
+
+    @classmethod
+    def read(cls, path, seqs):
+        s = cls()
+        rc = lib().rs_state_read(os.fsencode(path), C.byref(s.st), seqs._p)
+        if rc != RS_OK:
+            raise RSError(rc, "rs_state_read")
+        return s
+
+    @classmethod
+    def resume(cls, path_a, path_b, seqs):
+        s = cls()
+        which = C.c_int(-1)
+        r = lib().rs_state_resume(os.fsencode(path_a), os.fsencode(path_b), C.byref(s.st), seqs._p, C.byref(which))
+        return (s, which.value) if r == 1 else (None, -1)
+
+    def commit(self, path, seqs, factors):
+        f = np.ascontiguousarray(factors, dtype=FACTOR_DT).copy()
+        _check(lib().rs_factors_commit(os.fsencode(path), seqs._p, f.ctypes.data, len(f), C.byref(self.st)),
+               "rs_factors_commit")
+        return f
+
+    def finalize(self, path):
+        _check(lib().rs_factors_finalize(os.fsencode(path), C.byref(self.st)), "rs_factors_finalize")
+
+
+def verify_factor(p, k, n, c, base):
+    return lib().rs_verify_factor(p, k, n, c, base)
+
+
+def is_prime(n):
+    return bool(lib().rs_is_prime(n))
+
+
+def device_count():
+    return lib().rs_device_count()
+
+
+class Sieve:
+    """A device context running jobs (rs_ctx).  Raises when no CUDA device is present."""
+
+    def __init__(self, device=0):
+        L = lib()
+        self._c = C.c_void_p()
+        _check(L.rs_ctx_create(device, C.byref(self._c)), "rs_ctx_create")
+        self.seqs = None
+
+    def close(self):
+        if getattr(self, "_c", None) and self._c.value:
+            lib().rs_ctx_destroy(self._c)
+            self._c = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle):
+        _check(lib().rs_ctx_set_stream(self._c, C.c_void_p(stream_handle)), "rs_ctx_set_stream")
+
+    def load(self, seqs):
+        _check(lib().rs_job_load(self._c, seqs._p), "rs_job_load")
+        self.seqs = seqs
+
+    def run(self, p0, p1):
+        d = _Counters()
+        _check(lib().rs_run_range(self._c, p0, p1, C.byref(d)), "rs_run_range")
+        return {f: int(getattr(d, f)) for f in COUNTER_FIELDS}
+
+    def counters(self):
+        d = _Counters()
+        _check(lib().rs_counters_get(self._c, C.byref(d)), "rs_counters_get")
+        return {f: int(getattr(d, f)) for f in COUNTER_FIELDS}
+
+    def factors(self):
+        L = lib()
+        n = C.c_size_t(0)
+        rc = L.rs_factors_fetch(self._c, None, 0, C.byref(n))
+        if rc not in (RS_OK, RS_EARG):
+            _check(rc, "rs_factors_fetch")
+        out = np.zeros(max(n.value, 1), dtype=FACTOR_DT)
+        _check(L.rs_factors_fetch(self._c, out.ctypes.data, len(out), C.byref(n)), "rs_factors_fetch")
+        return out[: n.value].copy()
+
+    def bitmap(self):
+        s = self.seqs
+        out = np.zeros(s.kcount * s.words_per_seq, dtype=np.uint32)
+        _check(lib().rs_bitmap_download(self._c, out.ctypes.data, len(out)), "rs_bitmap_download")
+        return out.reshape(s.kcount, s.words_per_seq)
+
+    def primes(self, p0, p1, cap=None):
+        L = lib()
+        n = C.c_size_t(0)
+        if cap is None:
+            _check(L.rs_primes_generate(self._c, p0, p1, None, 0, C.byref(n)), "rs_primes_generate")
+            cap = n.value
+        out = np.zeros(max(cap, 1), dtype=np.uint64)
+        _check(L.rs_primes_generate(self._c, p0, p1, out.ctypes.data, cap, C.byref(n)), "rs_primes_generate")
+        return out[: n.value].copy()
+
+    def last_timing(self):
+        b, t = C.c_double(0), C.c_double(0)
+        bl, kl = C.c_uint32(0), C.c_uint32(0)
+        _check(lib().rs_last_timing(self._c, C.byref(b), C.byref(t), C.byref(bl), C.byref(kl)), "rs_last_timing")
+        return {"bsgs_ms_avg": b.value, "total_ms": t.value, "bsgs_launches": bl.value, "kernel_launches": kl.value}
+
+
+def term_set(factors):
+    """Eliminated terms (seq, n): what the reference README says to compare across runs."""
+    return set(zip(factors["seq"].tolist(), factors["n"].tolist()))

@@ -1,0 +1,195 @@
+// mont.cuh -- exact 64-bit modular arithmetic for sm_100a.
+//
+// Montgomery representation with R = 2^64: x is held as x*R mod p.  The
+// product is REDC(a*b) = a*b*R^-1 mod p with q = p^-1 mod 2^64, the same
+// reduction the reference uses (kernels/common.cl:33-40): because m*p agrees
+// with a*b in the low 64 bits, the result is hi(a*b) - hi(m*p), corrected by
+// +p when negative.  Valid for every odd p < 2^64 when a*b < p*2^64.
+//
+// The 64x64 products are written with 32-bit limbs and PTX carry chains
+// (mad.lo/hi.cc, madc) so that ptxas issues 32-bit IMADs with carry rather
+// than generic 64-bit multiply sequences.
+#pragma once
+#include <cstdint>
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+#define RS_DEV __device__ __forceinline__
+
+// hi64(a*b) and lo64(a*b), 32-bit limb schoolbook with carry propagation.
+RS_DEV void mul_wide(u64 a, u64 b, u64 &lo, u64 &hi)
+{
+    u32 a0 = (u32)a, a1 = (u32)(a >> 32), b0 = (u32)b, b1 = (u32)(b >> 32);
+    u32 t0, t1, t2, t3;
+    asm("{\n\t"
+        "mul.lo.u32      %0, %4, %6;\n\t"
+        "mul.hi.u32      %1, %4, %6;\n\t"
+        "mad.lo.cc.u32   %1, %5, %6, %1;\n\t"
+        "madc.hi.u32     %2, %5, %6, 0;\n\t"
+        "mad.lo.cc.u32   %1, %4, %7, %1;\n\t"
+        "madc.hi.cc.u32  %2, %4, %7, %2;\n\t"
+        "madc.hi.u32     %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32   %2, %5, %7, %2;\n\t"
+        "addc.u32        %3, %3, 0;\n\t"
+        "}"
+        : "=&r"(t0), "=&r"(t1), "=&r"(t2), "=&r"(t3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+    lo = ((u64)t1 << 32) | t0;
+    hi = ((u64)t3 << 32) | t2;
+}
+
+RS_DEV u64 mul_hi64(u64 a, u64 b)
+{
+    u64 lo, hi;
+    mul_wide(a, b, lo, hi);
+    return hi;
+}
+
+// Montgomery product: a*b*2^-64 mod p, result in [0,p).
+RS_DEV u64 mmul(u64 a, u64 b, u64 p, u64 q)
+{
+    u64 lo, hi;
+    mul_wide(a, b, lo, hi);
+    u64 m = lo * q;
+    u64 mp = mul_hi64(m, p);
+    u64 r = hi - mp;
+    return (hi < mp) ? r + p : r;
+}
+
+// a + b mod p for a, b in [0,p); correct for p up to 2^64-1 (wrapping add).
+RS_DEV u64 madd(u64 a, u64 b, u64 p)
+{
+    u64 c = (a >= p - b) ? p : 0;
+    return a + b - c;
+}
+
+RS_DEV u64 msub(u64 a, u64 b, u64 p) { return (a >= b) ? a - b : a - b + p; }
+RS_DEV u64 mneg(u64 a, u64 p) { return a ? p - a : 0; }
+
+// p^-1 mod 2^64 by Newton iteration: p*p == 1 mod 8 gives 3 correct bits,
+// each step doubles them (3, 6, 12, 24, 48, 96).
+RS_DEV u64 inv64(u64 p)
+{
+    u64 x = p;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) x *= 2 - p * x;
+    return x;
+}
+
+// 2^64 mod p for odd p >= 3 without a 64-bit division: reduce 2^64 - p' by
+// binary long division, where p' = p << s has its top bit set.
+RS_DEV u64 r_mod(u64 p)
+{
+    int s = __clzll(p);
+    u64 ps = p << s;              // ps in [2^63, 2^64)
+    u64 r = 0 - ps;               // 2^64 - ps < ps, and 2^64 == r (mod ps)
+    // r == 2^64 (mod ps) hence (mod p); now reduce r from < p*2^s to < p
+    for (int i = s - 1; i >= 0; --i) {
+        u64 t = p << i;
+        if (r >= t) r -= t;
+    }
+    return r;
+}
+
+// Montgomery constants of one prime.
+struct Mont {
+    u64 p, q, one, r2;
+};
+
+RS_DEV Mont mont_init(u64 p)
+{
+    Mont M;
+    M.p = p;
+    M.q = inv64(p);
+    M.one = r_mod(p);
+    // R^2 = (4R)^(2^5) in Montgomery form (4^32 = 2^64), as setup.cl:112-119
+    u64 two = madd(M.one, M.one, p);
+    u64 t = madd(two, two, p);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) t = mmul(t, t, p, M.q);
+    M.r2 = t;
+    return M;
+}
+
+RS_DEV u64 to_mont(u64 x, const Mont &M) { return mmul(x, M.r2, M.p, M.q); }   // any x < 2^64
+RS_DEV u64 from_mont(u64 x, const Mont &M) { return mmul(x, 1, M.p, M.q); }
+
+// x^e for a Montgomery x, left-to-right binary; e may be 0 or 1.
+RS_DEV u64 mpow(u64 x, u64 e, const Mont &M)
+{
+    if (e == 0) return M.one;
+    u64 a = x;
+    for (int bit = 62 - __clzll(e); bit >= 0; --bit) {
+        a = mmul(a, a, M.p, M.q);
+        if ((e >> bit) & 1) a = mmul(a, x, M.p, M.q);
+    }
+    return a;
+}
+
+// x * b mod p for a small integer multiplier b in [1, 16] by doubling and
+// adding (no multiply); the reference does the same for b = 2, 3, 5
+// (common.cl:74-85).  Larger b use mmul with the Montgomery form of b.
+RS_DEV u64 mul_small(u64 x, u32 b, u64 p)
+{
+    u64 acc = x;
+    int top = 31 - __clz(b);
+    for (int i = top - 1; i >= 0; --i) {
+        acc = madd(acc, acc, p);
+        if ((b >> i) & 1) acc = madd(acc, x, p);
+    }
+    return acc;
+}
+
+// Multiplication by the base: mul_small when b <= 16, else Montgomery.
+RS_DEV u64 mul_base(u64 x, u32 b, u64 bm, const Mont &M)
+{
+    return (b <= 16) ? mul_small(x, b, M.p) : mmul(x, bm, M.p, M.q);
+}
+
+// Jacobi symbol (a/n) for odd n > 0 and 0 <= a < n: binary algorithm
+// (strip factors of two with the (2/n) rule, swap with quadratic
+// reciprocity, subtract).  Returns -1, 0 or 1.
+RS_DEV int jacobi64(u64 a, u64 n)
+{
+    int t = 1;
+    while (a) {
+        int z = __ffsll((long long)a) - 1;
+        a >>= z;
+        u32 r8 = (u32)n & 7;
+        if ((z & 1) && (r8 == 3 || r8 == 5)) t = -t;
+        if (a < n) {
+            u64 tmp = a; a = n; n = tmp;
+            if ((a & 3) == 3 && (n & 3) == 3) t = -t;
+        }
+        a -= n;
+    }
+    return (n == 1) ? t : 0;
+}
+
+RS_DEV int jacobi32(u32 a, u32 n)
+{
+    int t = 1;
+    while (a) {
+        int z = __ffs((int)a) - 1;
+        a >>= z;
+        u32 r8 = n & 7;
+        if ((z & 1) && (r8 == 3 || r8 == 5)) t = -t;
+        if (a < n) {
+            u32 tmp = a; a = n; n = tmp;
+            if ((a & 3) == 3 && (n & 3) == 3) t = -t;
+        }
+        a -= n;
+    }
+    return (n == 1) ? t : 0;
+}
+
+// x mod d with a precomputed rd = floor((2^64-1)/d), d >= 1 (Barrett; the
+// estimate is short by at most 2).
+RS_DEV u64 mod_barrett(u64 x, u64 d, u64 rd)
+{
+    u64 qe = __umul64hi(x, rd);
+    u64 r = x - qe * d;
+    while (r >= d) r -= d;
+    return r;
+}

@@ -1,0 +1,117 @@
+// rs_internal.h -- device data layout shared by the kernels and the engine.
+//
+// Per job (a set of <= 100 sequences k_i*b^n+c_i sharing b, and an n-range)
+// the device holds a JobDev descriptor, the candidate bitmap and a factor
+// buffer.  Per segment of the p-range the device holds the generated primes;
+// per chunk of primes the setup kernel writes one record per prime (header,
+// power tables, BSGS targets) that the BSGS kernel consumes.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rs {
+
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+constexpr int KMAX = 100;            // sequences per job (inputfile.cpp:356-361)
+constexpr int KSTRIDE = 104;         // padded per-prime target stride
+constexpr int TABS = 128;            // u64 power-table entries per prime
+constexpr int NDS = 12;              // power-residue degrees of setup.cl:22-48
+
+// BSGS kernel shape: Q = BSGS_TPB * BSGS_C baby steps, NB buckets of 4 slots.
+constexpr int BSGS_TPB = 1024;
+constexpr int BSGS_C = 16;
+constexpr int BSGS_Q = BSGS_TPB * BSGS_C;   // 16384
+constexpr int BSGS_NBLOG = 13;              // 8192 buckets * 16 B = 128 KiB, load 1/2
+constexpr int BSGS_MAXPROBE = 64;
+
+constexpr int SETUP_TPB = 256;              // 8 primes (warps) per block
+constexpr int SIEVE_TPB = 512;
+constexpr int SIEVE_WORDS = 4096;           // 2^17 odd numbers per sieve block
+constexpr u64 MR_BOUND = 4295098369ULL;     // 65537^2: below it the sieve by all primes < 2^16 is exact
+
+// error bits (JobDev-independent, one word per context)
+constexpr u32 ERR_PRIME_OVERFLOW = 1u;      // segment produced more primes than the buffer holds
+constexpr u32 ERR_CAND_OVERFLOW = 2u;
+constexpr u32 ERR_HASH_OVERFLOW = 4u;       // a bucket chain exceeded BSGS_MAXPROBE
+constexpr u32 ERR_FACTOR_OVERFLOW = 8u;     // factor buffer full (cannot happen: sized to the bitmap)
+
+// statistics counters (u64)
+enum Stat {
+    ST_PRIMES = 0,        // primes generated (and tested)
+    ST_SKIPPED,           // primes dividing b or some k, or with no solvable k (setup.cl:156-162,205-208)
+    ST_FULL,              // primes searched with a full-range table (b a quadratic residue)
+    ST_PARITY,            // primes searched with a parity table (b a non-residue)
+    ST_TARGETS,           // sum over primes of surviving k
+    ST_BABY,              // baby steps executed
+    ST_GIANT,             // giant steps executed (one Montgomery product and one lookup each)
+    ST_SMALLORDER,        // primes with ord(b^e) < Q
+    ST_CANDIDATES,        // fingerprint matches verified
+    ST_HITS,              // verified solutions p | k*b^n+c with n in range
+    ST_FACTORS,           // bitmap claims won
+    ST_DUPS,              // solutions whose bitmap bit was already clear
+    ST_SIEVE_CANDS,       // sieve survivors given to Miller-Rabin
+    ST_COUNT
+};
+
+struct JobDev {
+    u32 base, kcount, nmin, nmax;
+    u32 L;               // nmax - nmin + 1
+    u32 words;           // bitmap words per sequence
+    u32 M1, M2;          // giant steps: ceil(L/Q) full, ceil(L/(2Q)) parity
+    u64 k[KMAX];
+    int c[KMAX];
+    u64 kodd[KMAX];      // odd part of k_i
+    u64 krd[KMAX];       // floor((2^64-1)/kodd)
+    u32 kv2[KMAX];       // 2-adic valuation of k_i
+    u64 bodd, brd;       // same for the base
+    u32 bv2;
+    u32 pad_;
+    u32 *bitmap;         // kcount * words
+};
+
+struct PrimeHdr {        // 64 bytes
+    u64 p;               // 0 = skipped
+    u64 q;               // p^-1 mod 2^64
+    u64 one;             // 2^64 mod p
+    u64 s;               // Montgomery b^e, e = 1 (full) or 2 (parity)
+    u64 S;               // Montgomery s^Q
+    u32 numk;            // surviving targets
+    u32 e;               // 1 or 2
+    u32 G, Lc;           // giant phase: G chunks of Lc giant steps
+    u32 smul;            // b^e as an integer when the baby step uses additions, else 0
+    u32 pad_;
+};
+
+struct FactorRec {       // one claimed term: p | k[seq]*b^n + c[seq]
+    u64 p;
+    u32 n;
+    u32 seq;
+};
+
+struct BsgsArgs {
+    u32 base, nmin, nmax, words;
+    u32 M1, M2;
+    u32 *bitmap;
+    FactorRec *factors;
+    u32 *factor_ctr;
+    u32 factor_cap;
+    u64 *stats;
+    u32 *err;
+};
+
+// launch wrappers (sieve.cu, setup.cu, bsgs.cu)
+cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp, u64 *cands, u32 cand_cap,
+                         u32 *ctrs, u32 *err, cudaStream_t st);
+cudaError_t launch_mr(const u64 *cands, const u32 *ctrs, u32 cand_cap, u64 *primes, u32 prime_cap, u32 *prime_ctr,
+                      u32 *err, int sms, cudaStream_t st);
+cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 count, PrimeHdr *hdr, void *aux, u64 *tabs,
+                         u64 *tgt, unsigned char *meta, u64 *stats, cudaStream_t st);
+size_t setup_aux_bytes();
+cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
+                        const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st);
+size_t bsgs_smem_bytes();
+cudaError_t bsgs_prepare();   // per device, before the first launch
+
+}  // namespace rs

@@ -1,0 +1,191 @@
+// sieve.cu -- sieve-prime generation over a segment [lo, hi) of the p-range.
+//
+// Replaces the reference's getsegprimes/addsmallprimes kernels
+// (kernels/getsegprimes.cl:128-182, kernels/addsmallprimes.cl:8-27, driven by
+// cl_sieve.cpp:1303-1320).  The reference emits base-2 strong probable primes
+// after removing multiples of 2..113; here each CTA runs a segmented
+// Eratosthenes sieve over 2^17 odd numbers in shared memory with every odd
+// prime below 2^16, compacts the survivors with warp ballots/popc, and a
+// second kernel proves the survivors at or above 65537^2 prime with the
+// 7-base strong-probable-prime test that verify_factor.c:100-128 uses
+// (deterministic below 2^64).  Survivors below 65537^2 are prime already.
+// The result is the exact set of odd primes in [lo, hi).
+#include "mont.cuh"
+#include "rs_internal.h"
+
+namespace rs {
+
+// x mod r for a 64-bit x and a 32-bit r, from three 32-bit remainders.
+__device__ __forceinline__ u32 mod64_32(u64 x, u32 r)
+{
+    u32 hi = (u32)(x >> 32), lo = (u32)x;
+    u32 t = (u32)(0u - r) % r;            // 2^32 mod r
+    u64 a = (u64)(hi % r) * t + (lo % r); // < r^2 + r < 2^33
+    return (u32)(a % r);
+}
+
+// One CTA sieves odd values base_odd + 2*i for i in [blk*BITS, blk*BITS+nbits).
+// ctrs[0] counts survivors written to cands.
+__global__ void __launch_bounds__(SIEVE_TPB) k_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *__restrict__ sp,
+                                                     u32 nsp, u64 *__restrict__ cands, u32 cand_cap, u32 *ctrs,
+                                                     u32 *err)
+{
+    constexpr u32 BITS = SIEVE_WORDS * 32;
+    __shared__ u32 bits[SIEVE_WORDS];
+    __shared__ u32 starts[7000];
+    const u32 tid = threadIdx.x;
+    const u64 i0 = (u64)blockIdx.x * BITS;
+    if (i0 >= nodd) return;
+    const u32 nbits = (u32)min((u64)BITS, nodd - i0);
+    const u64 bb = base_odd + 2 * i0;                   // value of bit 0 (odd)
+    const u64 vlast = bb + 2 * (u64)(nbits - 1);
+    for (u32 w = tid; w < SIEVE_WORDS; w += SIEVE_TPB) bits[w] = 0;
+
+    // first index to mark for each sieving prime r with r^2 <= vlast
+    u32 np_used = 0;
+    for (u32 k = tid; k < nsp; k += SIEVE_TPB) {
+        u32 r = sp[k];
+        u64 rr = (u64)r * r;
+        u32 s = 0xFFFFFFFFu;
+        if (rr <= vlast) {
+            u32 m = mod64_32(bb, r);
+            u32 j = (u32)(((u64)((r - m) % r) * ((r + 1) >> 1)) % r);   // bb + 2j == 0 (mod r)
+            u64 v = bb + 2 * (u64)j;
+            if (v < rr) j = (u32)((rr - bb) >> 1);                     // start at r^2, never at r
+            if ((u64)j < nbits) s = j;
+        }
+        starts[k] = s;
+    }
+    // number of primes with r^2 <= vlast (sp is ascending)
+    {
+        u32 lo = 0, hi2 = nsp;
+        while (lo < hi2) {
+            u32 mid = (lo + hi2) >> 1;
+            if ((u64)sp[mid] * sp[mid] <= vlast) lo = mid + 1; else hi2 = mid;
+        }
+        np_used = lo;
+    }
+    __syncthreads();
+
+    // small primes: all threads stride over the multiples of one prime
+    u32 k = 0;
+    for (; k < np_used && sp[k] < 2 * SIEVE_TPB; ++k) {
+        u32 r = sp[k], s = starts[k];
+        if (s == 0xFFFFFFFFu) continue;
+        for (u32 i = s + tid * r; i < nbits; i += SIEVE_TPB * r) atomicOr(&bits[i >> 5], 1u << (i & 31));
+    }
+    // large primes: one prime per thread
+    for (u32 kk = k + tid; kk < np_used; kk += SIEVE_TPB) {
+        u32 r = sp[kk], s = starts[kk];
+        for (u32 i = s; i < nbits; i += r) atomicOr(&bits[i >> 5], 1u << (i & 31));
+    }
+    __syncthreads();
+
+    // warp-ballot / popc compaction of the unmarked (prime or MR-candidate) values
+    const u32 lane = tid & 31;
+    const u32 nw = (nbits + 31) >> 5;
+    for (u32 w0 = 0; w0 < SIEVE_WORDS; w0 += SIEVE_TPB) {
+        u32 w = w0 + tid;
+        u32 live = 0;
+        if (w < nw) {
+            live = ~bits[w];
+            u32 rem = nbits - w * 32;
+            if (rem < 32) live &= (1u << rem) - 1;
+        }
+        u32 cnt = __popc(live);
+        u32 incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            u32 v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= (u32)o) incl += v;
+        }
+        u32 total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        u32 basepos = 0;
+        if (lane == 31 && total) basepos = atomicAdd(&ctrs[0], total);
+        basepos = __shfl_sync(0xFFFFFFFFu, basepos, 31);
+        if (total == 0) continue;
+        u32 pos = basepos + incl - cnt;
+        if (basepos + total > cand_cap) {
+            if (lane == 0) atomicOr(err, ERR_CAND_OVERFLOW);
+            continue;
+        }
+        while (live) {
+            u32 b = __ffs(live) - 1;
+            live &= live - 1;
+            cands[pos++] = bb + 2 * (u64)(w * 32 + b);
+        }
+    }
+}
+
+// Deterministic primality below 2^64: the seven strong-probable-prime bases
+// of verify_factor.c:102.
+__device__ bool is_prime_mr(u64 n)
+{
+    if (n < MR_BOUND) return true;        // sieve survivor below 65537^2
+    const u32 bases[7] = {2u, 325u, 9375u, 28178u, 450775u, 9780504u, 1795265022u};
+    Mont M = mont_init(n);
+    const u64 nm1 = n - 1;
+    const int t = __ffsll((long long)nm1) - 1;
+    const u64 d = nm1 >> t;
+    const u64 mone = n - M.one;           // Montgomery form of -1
+    for (int i = 0; i < 7; ++i) {
+        u64 a = bases[i];                 // every base is below n >= 65537^2
+        u64 x = mpow(to_mont(a, M), d, M);
+        if (x == M.one || x == mone) continue;
+        bool ok = false;
+        for (int s = 1; s < t; ++s) {
+            x = mmul(x, x, n, M.q);
+            if (x == mone) { ok = true; break; }
+        }
+        if (!ok) return false;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_mr(const u64 *__restrict__ cands, const u32 *__restrict__ ctrs,
+                                            u32 cand_cap, u64 *__restrict__ primes, u32 prime_cap, u32 *prime_ctr,
+                                            u32 *err)
+{
+    const u32 n = min(ctrs[0], cand_cap);
+    const u32 lane = threadIdx.x & 31;
+    const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 b0 = warp * 32; b0 < n; b0 += nwarps * 32) {
+        u32 idx = b0 + lane;
+        u64 v = 0;
+        bool pr = false;
+        if (idx < n) {
+            v = cands[idx];
+            pr = is_prime_mr(v);
+        }
+        u32 mask = __ballot_sync(0xFFFFFFFFu, pr);
+        if (!mask) continue;
+        u32 basepos = 0;
+        if (lane == 0) basepos = atomicAdd(prime_ctr, __popc(mask));
+        basepos = __shfl_sync(0xFFFFFFFFu, basepos, 0);
+        if (basepos + __popc(mask) > prime_cap) {
+            if (lane == 0) atomicOr(err, ERR_PRIME_OVERFLOW);
+            continue;
+        }
+        if (pr) primes[basepos + __popc(mask & ((1u << lane) - 1))] = v;
+    }
+}
+
+cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp, u64 *cands, u32 cand_cap, u32 *ctrs,
+                         u32 *err, cudaStream_t st)
+{
+    if (nodd == 0) return cudaSuccess;
+    constexpr u64 BITS = (u64)SIEVE_WORDS * 32;
+    u64 blocks = (nodd + BITS - 1) / BITS;
+    k_sieve<<<(unsigned)blocks, SIEVE_TPB, 0, st>>>(base_odd, nodd, hi, sp, nsp, cands, cand_cap, ctrs, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mr(const u64 *cands, const u32 *ctrs, u32 cand_cap, u64 *primes, u32 prime_cap, u32 *prime_ctr,
+                      u32 *err, int sms, cudaStream_t st)
+{
+    k_mr<<<sms * 8, 256, 0, st>>>(cands, ctrs, cand_cap, primes, prime_cap, prime_ctr, err);
+    return cudaGetLastError();
+}
+
+}  // namespace rs

@@ -1,0 +1,80 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Bit-exact integer work: prime sets, eliminated-term sets and final bitmaps
+must be identical to the brute-force oracle (which evaluates k*b^n mod p for
+every prime and n) on the same seeded inputs.
+"""
+import numpy as np
+import pytest
+
+from rssieve_b200 import workloads as W
+from tests.conftest import oracle_job
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("lo,hi", [
+    (3, 2_000_000),                                   # exact sieve region, tiny primes
+    (4_294_000_000, 4_296_500_000),                   # across 2^32 and 65537^2 (Miller-Rabin starts)
+    (1 << 50, (1 << 50) + 30_000_000),                # config 2 region
+    (10 ** 12, 10 ** 12 + 20_000_000),                # config 1 region
+    ((1 << 64) - (1 << 27), (1 << 64) - 1),           # just below 2^64 (config 4 region)
+    (1_000_003, 1_000_004),                           # single odd number, prime
+    (1_000_004, 1_000_005),                           # single even number
+])
+def test_primes_match_oracle(sieve, oracle, lo, hi):
+    got = np.sort(sieve.primes(lo, hi))
+    want = oracle.primes(lo, hi)
+    assert got.dtype == np.uint64
+    assert len(got) == len(want)
+    assert np.array_equal(got, want)
+
+
+def _check_job(sieve, oracle, job, p0, p1, rs):
+    seqs = W.seqs_of(job)
+    sieve.load(seqs)
+    cnt = sieve.run(p0, p1)
+    fac = sieve.factors()
+    bm = sieve.bitmap()
+    oj = oracle_job(oracle, job)
+    plist = oracle.primes(p0, p1)
+    ofac, odups, obm = oracle.brute(oj, plist, ref_skip=True)
+    assert oracle.term_set(fac) == oracle.term_set(ofac)
+    assert np.array_equal(bm, obm)
+    assert cnt["primes"] == len(plist)
+    assert cnt["factors"] == len(fac)
+    assert cnt["dups"] == odups
+    # every reported factor is a real one, by the host verifier
+    for f in fac[:2000]:
+        seq = int(f["seq"])
+        assert rs.verify_factor(int(f["p"]), job["k"][seq], int(f["n"]), job["c"][seq], job["base"]) == 1
+    return cnt, fac
+
+
+@pytest.mark.parametrize("seed,base", [(11, 2), (12, 3), (13, 5), (14, 6), (15, 10), (16, 7)])
+def test_small_p_dense_factors(sieve, oracle, rs, seed, base):
+    """p from 3: small orders, p dividing k, many duplicates and claims."""
+    job = W.small_job(seed, kcount=12, base=base, nmin=1000, nmax=9000, keep=0.4, kmax=1 << 24)
+    _check_job(sieve, oracle, job, 3, 300_000, rs)
+
+
+def test_config1_shape_high_density_window(sieve, oracle, rs):
+    job = W.small_job(21, kcount=8, base=2, nmin=100000, nmax=140000, keep=0.06, kmax=1 << 20, signs=-1)
+    _check_job(sieve, oracle, job, 10 ** 6, 10 ** 6 + 400_000, rs)
+
+
+def test_hundred_sequences_mid_p(sieve, oracle, rs):
+    job = W.small_job(22, kcount=100, base=2, nmin=20000, nmax=80000, keep=0.05, kmax=1 << 32)
+    _check_job(sieve, oracle, job, 5 * 10 ** 7, 5 * 10 ** 7 + 200_000, rs)
+
+
+def test_odd_nmin_parity_offsets(sieve, oracle, rs):
+    job = W.small_job(23, kcount=10, base=2, nmin=3001, nmax=12000, keep=0.5, kmax=1 << 24)
+    _check_job(sieve, oracle, job, 1000, 200_000, rs)
+
+
+def test_large_k_near_2_64(sieve, oracle, rs):
+    """config 4 shape on a narrow window: b=5, k < 2^40, p just below 2^64."""
+    job = W.small_job(24, kcount=20, base=5, nmin=1000, nmax=200000, keep=0.05, kmax=1 << 40)
+    lo = (1 << 64) - (1 << 22)
+    _check_job(sieve, oracle, job, lo, (1 << 64) - 1, rs)
