@@ -1,0 +1,295 @@
+"""Benchmark: primes tested/s of the plain BSGS sieve on the 100-sequence job.
+
+Workload (config 2): 100 sequences k*2^n+-1 (50 with +1, 50 with -1), k odd
+in [3,2^32), n in [4e6,1e7) kept with probability 0.03 (seeded synthetic
+bitmap, ~1.8e7 candidate terms), sieved over consecutive windows of the
+p-range [2^50, 2^50+2^38).  One step = one rs_run_range call over a window of
+width --width (default 2^29, ~1.5e7 primes): prime generation, per-prime
+set-up and the BSGS search, with factors accumulating on the device.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--width BITS] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): each rank sieves its own disjoint
+windows (weak scaling, no data-path collective); the timed region is bracketed
+by barriers and the max over ranks is reported.  `value` counts inputs already
+resident in HBM; `e2e` runs the same windows through the C ABI with the job's
+host buffers (pinned) uploaded and the factors downloaded every step.
+--impl reference times the CPU port of the reference algorithm (oracle/,
+kind "port": the reference ships only OpenCL kernels, no CPU path) on a
+bounded sample of the same workload with every host thread.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "primes tested/s at 100 seqs, batched vs plain on 1 B200; p50/p99 unit latency"
+WORKLOAD = ("config2 plain form: 100 seqs k*2^n+-1 (50 +1, 50 -1), k odd U[3,2^32), n in [4e6,1e7) "
+            "kept w.p. 0.03, p windows from 2^50")
+P_START = 1 << 50
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--width", type=int, default=29, help="log2 of the p-window per step")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, gpu):
+        self.path = os.path.join("/tmp", "rs_clocks_%d_%d.csv" % (os.getpid(), gpu))
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.fh = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in open(self.path):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(seed, target_s, job=None):
+    """The oracle's CPU port of the reference BSGS algorithm on a bounded sample of the workload."""
+    from oracle import pyoracle as O
+    from rssieve_b200 import workloads as W
+    job = job or W.config2(seed)
+    oj = O.Job(job["base"], job["k"], job["c"], job["nmin"], job["nmax"], job["bitmap"])
+    threads = os.cpu_count() or 1
+    pl = O.prp2(P_START, P_START + 400_000)           # the reference's own prime set (2-PRPs)
+    t = time.perf_counter()
+    O.bsgs(oj, pl[: 64 * threads], nthreads=threads)
+    pilot = 64 * threads / max(time.perf_counter() - t, 1e-6)
+    want = int(min(max(pilot * target_s, 32 * threads), 2_000_000))
+    width = int(want * 36.0) + 1000
+    pl = O.prp2(P_START, P_START + width)[:want]
+    t = time.perf_counter()
+    f, st, _ = O.bsgs(oj, pl, nthreads=threads)
+    dt = time.perf_counter() - t
+    return {"value": len(pl) / dt, "unit": "primes/s", "cores": threads, "kind": "port",
+            "sample": "%d 2-PRPs from 2^50 (config2 job), %d threads, %.1f s; %.3g Montgomery products/s" % (
+                len(pl), threads, dt, st["mulmods"] / dt)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    res = []
+    from rssieve_b200 import workloads as W
+    job = W.config2(args.seed)
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(args.seed, max(2.0, args.cpu_seconds / 2), job)
+        if i >= args.warmup:
+            res.append(r)
+    v = statistics.median(r["value"] for r in res)
+    line = {"metric": METRIC, "value": v, "unit": "primes/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "p_window": "bounded CPU sample from 2^50"},
+            "cpu_baseline": {"value": v, "unit": "primes/s", "cores": res[0]["cores"], "kind": "port",
+                             "sample": res[-1]["sample"]},
+            "e2e": {"value": v, "unit": "primes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import numpy as np
+    import rssieve_b200 as rs
+    from rssieve_b200 import workloads as W
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+        return float(t.item())
+
+    job = W.config2(args.seed)
+    seqs = W.seqs_of(job)
+    stream = torch.cuda.current_stream()
+    sv = rs.Sieve(local)
+    sv.set_stream(stream.cuda_stream)
+    peak = sv.mulmod_peak()
+    sv.load(seqs)
+    width = 1 << args.width
+    # disjoint windows per rank: rank r takes windows r, r+world, ...
+    nwin = args.warmup + args.steps
+    windows = [(P_START + (i * world + rank) * width, P_START + (i * world + rank + 1) * width) for i in range(nwin)]
+    l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    for i in range(args.warmup):
+        sv.run(*windows[i])
+    sv.factors()
+    torch.cuda.synchronize()
+    barrier()
+
+    clk = Clocks(local)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    tot = {}
+    bsgs_ms, bsgs_launches, kernel_launches = 0.0, 0, 0
+    barrier()
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    for i in range(args.steps):
+        l2_flush.zero_()                               # flush L2 between steps (outside the step events)
+        evs[i][0].record(stream)
+        c = sv.run(*windows[args.warmup + i])
+        evs[i][1].record(stream)
+        tm = sv.last_timing()
+        bsgs_ms += tm["bsgs_ms_avg"] * tm["bsgs_launches"]
+        bsgs_launches += tm["bsgs_launches"]
+        kernel_launches += tm["kernel_launches"]
+        for k, v in c.items():
+            tot[k] = tot.get(k, 0) + v
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - t_wall
+    clocks = clk.stop()
+    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    dev_ms_max = max_over_ranks(dev_ms)
+    primes_all = sum_over_ranks(tot["primes"])
+    value = primes_all / (dev_ms_max / 1e3)
+    giant_all = sum_over_ranks(tot["giant"])
+    bsgs_ms_avg = bsgs_ms / max(bsgs_launches, 1)
+    # roofline of the BSGS kernel: giant-step Montgomery products per launch / average launch time
+    achieved = (tot["giant"] / max(bsgs_launches, 1)) / (bsgs_ms_avg / 1e3) / 1e9
+    fac = sv.factors()
+
+    e2e = None
+    if not args.no_e2e:
+        # end to end through the C ABI: pinned host job -> device each step, factors -> host each step
+        bm = seqs.bitmap
+        cudart = torch.cuda.cudart()
+        cudart.cudaHostRegister(bm.ctypes.data, bm.nbytes, 0)
+        ewin = [(P_START + ((nwin + i) * world + rank) * width, P_START + ((nwin + i) * world + rank + 1) * width)
+                for i in range(args.steps)]
+        sv.load(seqs)
+        sv.run(*ewin[0])                               # warm the load/run/fetch path once
+        sv.factors()
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eprimes, d2h = 0, 0
+        for i in range(args.steps):
+            sv.load(seqs)
+            c = sv.run(*ewin[i])
+            f = sv.factors()
+            eprimes += c["primes"]
+            d2h += len(f) * 16 + 13 * 8
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = max_over_ranks(e0.elapsed_time(e1))
+        cudart.cudaHostUnregister(bm.ctypes.data)
+        e2e = {"value": sum_over_ranks(eprimes) / (ems / 1e3), "unit": "primes/s",
+               "h2d_bytes_per_step": int(bm.nbytes + 2400), "d2h_bytes_per_step": int(d2h / args.steps)}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_baseline(args.seed, args.cpu_seconds, job)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "primes/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "p_window_log2": args.width, "seed": args.seed,
+                       "l2": "flushed between steps (256 MiB write outside the step events)",
+                       "parallelism": "p-range windows per rank" if world > 1 else "1 GPU"},
+            "e2e": e2e,
+            "gpu_launches": kernel_launches,
+            "roofline": {"bound": "int32-imad (64-bit Montgomery products)", "achieved": achieved, "peak": peak,
+                         "unit": "Gmulmod/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured live: rs_mulmod_peak, independent Montgomery-product chains"},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "detail": {"primes": tot["primes"], "giant_steps": tot["giant"], "baby_steps": tot["baby"],
+                       "targets_per_prime": tot["targets"] / max(tot["full"] + tot["parity"], 1),
+                       "giant_per_prime": tot["giant"] / max(tot["primes"], 1),
+                       "skipped": tot["skipped"], "factors": int(len(fac)), "dups": tot["dups"],
+                       "candidates": tot["candidates"], "bsgs_ms_avg": bsgs_ms_avg,
+                       "bsgs_share": bsgs_ms / max(dev_ms, 1e-9), "wall_s": wall,
+                       "mont_products_per_s": giant_all / (dev_ms_max / 1e3)},
+        }
+        print(json.dumps(line), flush=True)
+    sv.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

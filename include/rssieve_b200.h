@@ -163,6 +163,11 @@ int rs_primes_generate(rs_ctx *ctx, uint64_t p0, uint64_t p1, uint64_t *dst, siz
 int rs_last_timing(rs_ctx *ctx, double *bsgs_ms, double *total_kernel_ms, uint32_t *bsgs_launches,
                    uint32_t *kernel_launches);
 
+/* Throughput of independent 64-bit Montgomery products (the kernels' mmul)
+ * on this device, in 10^9 products/s: the roofline denominator of the
+ * integer-multiply-bound BSGS kernel. */
+int rs_mulmod_peak(rs_ctx *ctx, double *gmulmods_per_s, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -344,11 +344,16 @@ size_t or_brute(or_job *job, const uint64_t *primes, size_t np, int ref_skip,
     size_t cnt = 0;
     uint64_t dup = 0;
     const uint32_t K = job->kcount;
-    for (size_t ip = 0; ip < np; ++ip) {
+    /* primes run in parallel: claims are atomic, so the eliminated-term set,
+     * the final bitmap and the duplicate count do not depend on the order */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : dup) if (np > 64)
+#endif
+    for (long long ip = 0; ip < (long long)np; ++ip) {
         uint64_t p = primes[ip];
         if (p < 3 || !(p & 1)) continue;
         uint64_t bm = job->base % p;
-        if (bm == 0) continue;                       /* b^n = 0: no term divisible */
+        if (bm == 0) continue;                       /* b^n = 0: no term is divisible */
         /* targets b^n == -c_i * k_i^-1 (mod p), as Montgomery residues */
         uint64_t q = or_invert(p), one = (0 - p) % p, r2 = r2_of(p, q, one);
         uint64_t tv[256]; int16_t ts[256]; uint8_t used[256];

@@ -64,7 +64,7 @@ size_t or_prp2(uint64_t lo, uint64_t hi, uint64_t *out, size_t cap);    /* refer
 int or_verify_factor(uint64_t p, uint64_t k, uint32_t n, int32_t c, uint32_t base);
 
 /* ---- brute-force term oracle ----
- * primes must be ascending.  For every prime and every n in [nmin,nmax] it
+ * For every prime (run in parallel) and every n in [nmin,nmax] it
  * evaluates b^n mod p and claims the bitmap bit of every term p | k*b^n+c.
  * ref_skip != 0 applies the reference's rule that a prime dividing b or any k
  * is skipped for all sequences (setup.cl:156-162).

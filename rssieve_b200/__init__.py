@@ -50,7 +50,7 @@ EXPORTS = (
     "rs_factors_file_apply", "rs_factors_commit", "rs_factors_finalize", "rs_state_write", "rs_state_read",
     "rs_state_resume", "rs_ctx_create", "rs_ctx_destroy", "rs_ctx_set_stream", "rs_device_count",
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
-    "rs_primes_generate", "rs_last_timing",
+    "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak",
 )
 
 _lib = None
@@ -97,6 +97,7 @@ def lib():
         "rs_primes_generate": (C.c_int, [vp, u64, u64, vp, sz, C.POINTER(sz)]),
         "rs_last_timing": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(u32),
                                      C.POINTER(u32)]),
+        "rs_mulmod_peak": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -309,6 +310,12 @@ class Sieve:
         out = np.zeros(max(cap, 1), dtype=np.uint64)
         _check(L.rs_primes_generate(self._c, p0, p1, out.ctypes.data, cap, C.byref(n)), "rs_primes_generate")
         return out[: n.value].copy()
+
+    def mulmod_peak(self):
+        """10^9 Montgomery products/s of independent chains on this device."""
+        g, ms = C.c_double(0), C.c_double(0)
+        _check(lib().rs_mulmod_peak(self._c, C.byref(g), C.byref(ms)), "rs_mulmod_peak")
+        return g.value
 
     def last_timing(self):
         b, t = C.c_double(0), C.c_double(0)

@@ -113,5 +113,6 @@ cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs,
                         const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st);
 size_t bsgs_smem_bytes();
 cudaError_t bsgs_prepare();   // per device, before the first launch
+cudaError_t launch_mulmod_peak(u64 *out, int blocks, int iters, cudaStream_t st);
 
 }  // namespace rs
