@@ -8,8 +8,9 @@
 //                ord(s) < Q (giant.cl:123-134), then inserts j < ord into a
 //                shared-memory hash table.
 //   giant phase  gamma = T_i * S^q for q in [0,M): thread (i,g) walks q in
-//                [g*Lc, (g+1)*Lc) from T_i * S^(g*Lc), one Montgomery product
-//                and one table probe per step (giant.cl:170-192).  A match
+//                [g*Lc, (g+1)*Lc) from T_i * S^(g*Lc) as two interleaved
+//                chains, one Montgomery product and one table probe per step
+//                (giant.cl:170-192).  A match
 //                s^j == gamma gives n = nmin + off_i + e*((q+1)*Q - 1 - j).
 //   small order  ord(s) < Q: each target is looked up once and every n in
 //                range with the same residue mod e*ord is claimed (giant.cl:146-168).
@@ -17,9 +18,9 @@
 //                {p, n, seq} to the factor buffer (giant.cl:21-39,158-162).
 //
 // Hash table: NB buckets of four 32-bit slots in shared memory (load 1/2).
-// A slot holds a 16-bit fingerprint (high half of lo32(y)*0x9E3779B1), j+1 in
-// bits 1..15 and, in slot 3, an overflow flag in bit 0 that tells a probe to
-// continue into the next bucket.  The bucket is lo32(y) mod NB.  A fingerprint
+// A slot holds a 16-bit fingerprint of y, j+1 in bits 1..15 and, in slot 3, an
+// overflow flag in bit 0 that tells a probe to continue into the next bucket
+// (see tab_hash for the bucket and fingerprint).  A fingerprint
 // match is verified exactly by recomputing y_j from its thread's start value,
 // so the search is exact for every 64-bit value (the reference's split
 // lo32/hi32 table cannot find values whose low 32 bits are zero, giant.cl:46,63).
@@ -30,36 +31,53 @@ namespace rs {
 
 constexpr u32 HMUL = 0x9E3779B1u;
 
-template <u32 NB>
+// Table hash of a 64-bit residue: h = (lo32 ^ hi32) * 0x9E3779B1.  The bucket
+// is the top NBLOG bits of h and the 16-bit fingerprint the bits below them.
+// Both words are folded in because the baby chain for small bases is a run of
+// doublings (x -> 2x mod p): the low bits alone repeat shifted patterns and
+// crowd a few buckets.
+template <u32 NBLOG>
+__device__ __forceinline__ void tab_hash(u64 val, u32 &bucket, u32 &key)
+{
+    const u32 h = ((u32)val ^ (u32)(val >> 32)) * HMUL;
+    bucket = h >> (32 - NBLOG);
+    key = (h << NBLOG) & 0xFFFF0000u;
+}
+
+template <u32 NBLOG>
 __device__ __forceinline__ void tab_insert(uint4 *table, u64 val, u32 j, u32 *err)
 {
-    const u32 lo = (u32)val;
-    u32 b = lo & (NB - 1);
-    const u32 ent = ((lo * HMUL) & 0xFFFF0000u) | ((j + 1) << 1);
-    for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
+    constexpr u32 NB = 1u << NBLOG;
+    u32 b, key;
+    tab_hash<NBLOG>(val, b, key);
+    const u32 ent = key | ((j + 1) << 1);
+    for (int pr = 0; pr < BSGS_MAXPROBE;) {
         u32 *sl = reinterpret_cast<u32 *>(&table[b]);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            u32 old = reinterpret_cast<volatile u32 *>(sl)[k];
-            while ((old >> 1) == 0) {
-                const u32 prev = atomicCAS(&sl[k], old, old | ent);
-                if (prev == old) return;
-                old = prev;
-            }
+        u32 cur[4];
+        asm volatile("ld.volatile.shared.v4.u32 {%0,%1,%2,%3}, [%4];"
+                     : "=r"(cur[0]), "=r"(cur[1]), "=r"(cur[2]), "=r"(cur[3])
+                     : "r"((u32)__cvta_generic_to_shared(sl)));
+        int k = 0;
+        while (k < 4 && (cur[k] >> 1) != 0) ++k;
+        if (k < 4) {
+            // slots only ever fill, so a stale 'empty' just fails the CAS; re-read then
+            if (atomicCAS(&sl[k], cur[k], cur[k] | ent) == cur[k]) return;
+            continue;
         }
         atomicOr(&sl[3], 1u);                // bucket full: mark overflow, go on
         b = (b + 1) & (NB - 1);
+        ++pr;
     }
     atomicOr(err, ERR_HASH_OVERFLOW);
 }
 
 // Calls f(j) for every slot whose fingerprint matches val.
-template <u32 NB, class F>
+template <u32 NBLOG, class F>
 __device__ __forceinline__ void tab_probe(const uint4 *table, u64 val, F &&f)
 {
-    const u32 lo = (u32)val;
-    u32 b = lo & (NB - 1);
-    const u32 key = (lo * HMUL) & 0xFFFF0000u;
+    constexpr u32 NB = 1u << NBLOG;
+    u32 b, key;
+    tab_hash<NBLOG>(val, b, key);
     for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
         const uint4 bv = table[b];
         if (((bv.x ^ key) < 0x10000u) && (bv.x & 0xFFFEu)) f(((bv.x >> 1) & 0x7FFFu) - 1);
@@ -158,7 +176,7 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
 #pragma unroll
         for (int i = 0; i < C; ++i) {
             const u32 j = tid * C + i;
-            if (j < order) tab_insert<NB>(table, v[i], j, a.err);
+            if (j < order) tab_insert<NBLOG>(table, v[i], j, a.err);
         }
         __syncthreads();
 
@@ -172,31 +190,46 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
 
         const u32 Mg = (e == 2) ? a.M2 : a.M1;
         if (order == 0xFFFFFFFFu) {
-            // ---- giant steps ----
+            // ---- giant steps: two independent chains per thread ----
+            // chain A walks q in [q0, q0+h), chain B q in [q0+h, q1), h = Lc/2;
+            // B starts from A's start times S^h (H.Sh), so the two Montgomery
+            // products of a step are independent and overlap in the pipeline.
             const u32 G = H.G, Lc = H.Lc;
             if (tid < numk * G) {
                 const u32 i = tid / G, g = tid - i * G;
                 const u32 q0 = g * Lc;
                 const u32 q1 = min(q0 + Lc, Mg);
+                const u32 h = Lc >> 1;
+                const u32 nA = min(h, q1 - q0), nB = (q1 - q0) - nA;
                 const u32 m = s_meta[i];
                 const u32 seq = m & 0x7Fu, off = m >> 7;
-                u64 gamma = mmul(s_T[i], s_Z[g], p, q);
-                for (u32 qq = q0; qq < q1; ++qq) {
-                    tab_probe<NB>(table, gamma, [&](u32 j) {
-                        atomicAdd(&s_cands, 1u);
-                        if (!verify(j, gamma)) return;
-                        const u64 u = (u64)(qq + 1) * Q - 1 - j;
-                        const u64 n = (u64)a.nmin + off + (u64)e * u;
-                        if (n <= a.nmax) claim(a, p, seq, (u32)n, &s_dups, &s_facs);
-                    });
-                    gamma = mmul(gamma, S, p, q);
+                u64 gA = mmul(s_T[i], s_Z[g], p, q);
+                u64 gB = mmul(gA, H.Sh, p, q);
+                auto hit = [&](u32 qq, u32 j, u64 gamma) {
+                    atomicAdd(&s_cands, 1u);
+                    if (!verify(j, gamma)) return;
+                    const u64 u = (u64)(qq + 1) * Q - 1 - j;
+                    const u64 n = (u64)a.nmin + off + (u64)e * u;
+                    if (n <= a.nmax) claim(a, p, seq, (u32)n, &s_dups, &s_facs);
+                };
+                for (u32 t = 0; t < nB; ++t) {
+                    if (t < nA) {
+                        const u32 qa = q0 + t;
+                        const u64 ga = gA;
+                        tab_probe<NBLOG>(table, ga, [&](u32 j) { hit(qa, j, ga); });
+                        gA = mmul(gA, S, p, q);
+                    }
+                    const u32 qb = q0 + h + t;
+                    const u64 gb = gB;
+                    tab_probe<NBLOG>(table, gb, [&](u32 j) { hit(qb, j, gb); });
+                    gB = mmul(gB, S, p, q);
                 }
             }
         } else {
             // ---- ord(s) < Q: one lookup per target ----
             if (tid < numk) {
                 const u64 T = s_T[tid];
-                tab_probe<NB>(table, T, [&](u32 j) {
+                tab_probe<NBLOG>(table, T, [&](u32 j) {
                     atomicAdd(&s_cands, 1u);
                     if (j >= order || !verify(j, T)) return;
                     const u32 k = atomicAdd(&s_nsol, 1u);

@@ -18,7 +18,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/rssieve_b200.h"
+#include "rssieve_b200.h"
 
 #define STATE_A "stateA.ckp"
 #define STATE_B "stateB.ckp"

@@ -1,6 +1,6 @@
 // rs_host.h -- internal helpers shared by the host services and the engine.
 #pragma once
-#include "../../include/rssieve_b200.h"
+#include "rssieve_b200.h"
 
 #ifdef __cplusplus
 extern "C" {

@@ -71,7 +71,7 @@ struct JobDev {
     u32 *bitmap;         // kcount * words
 };
 
-struct PrimeHdr {        // 64 bytes
+struct PrimeHdr {        // 72 bytes
     u64 p;               // 0 = skipped
     u64 q;               // p^-1 mod 2^64
     u64 one;             // 2^64 mod p
@@ -82,6 +82,7 @@ struct PrimeHdr {        // 64 bytes
     u32 G, Lc;           // giant phase: G chunks of Lc giant steps
     u32 smul;            // b^e as an integer when the baby step uses additions, else 0
     u32 pad_;
+    u64 Sh;              // Montgomery S^(Lc/2): start of a thread's second giant chain
 };
 
 struct FactorRec {       // one claimed term: p | k[seq]*b^n + c[seq]

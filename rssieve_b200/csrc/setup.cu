@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
     const u64 p = primes[first + t];
     PrimeHdr H;
     H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.pad_ = 0;
+    H.Sh = 0;
     const Mont M = mont_init(p);
     const u32 b = job->base;
     const u64 bm = to_mont(b, M);
@@ -208,10 +209,12 @@ __global__ void __launch_bounds__(SETUP_TPB) k_setup_k(const JobDev *__restrict_
     u64 *tb = tabs + (size_t)w * TABS;
     tb[64 + lane] = acc;
     tb[96 + lane] = acc2;
+    const u64 sh = mpow(H.S, (u64)(Lc >> 1), M);
     if (lane == 0) {
         hdr[w].numk = nk;
         hdr[w].G = G;
         hdr[w].Lc = Lc;
+        hdr[w].Sh = sh;
         atomicAdd(&stats[ST_TARGETS], (u64)nk);
         atomicAdd(&stats[H.e == 2 ? ST_PARITY : ST_FULL], 1ull);
     }
