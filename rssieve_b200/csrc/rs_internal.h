@@ -15,7 +15,7 @@ typedef unsigned long long u64;
 typedef unsigned int u32;
 
 constexpr int KMAX = 100;            // sequences per job (inputfile.cpp:356-361)
-constexpr int KSTRIDE = 104;         // padded per-prime target stride
+constexpr int KSTRIDE = 112;         // padded per-prime target stride (16-byte multiple for bulk copies)
 constexpr int TABS = 128;            // u64 power-table entries per prime
 constexpr int NDS = 12;              // power-residue degrees of setup.cl:22-48
 
@@ -25,6 +25,7 @@ constexpr int BSGS_C = 16;
 constexpr int BSGS_Q = BSGS_TPB * BSGS_C;   // 16384
 constexpr int BSGS_NBLOG = 13;              // 8192 buckets * 16 B = 128 KiB, load 1/2
 constexpr int BSGS_MAXPROBE = 64;
+constexpr int BSGS_SPEC_PROBE = 64;        // bucket walk bound while ord(s) is still unknown (walks of 17 occur about once per 10^4 primes)
 
 constexpr int SETUP_TPB = 256;              // 8 primes (warps) per block
 constexpr int SIEVE_TPB = 512;
@@ -36,6 +37,7 @@ constexpr u32 ERR_PRIME_OVERFLOW = 1u;      // segment produced more primes than
 constexpr u32 ERR_CAND_OVERFLOW = 2u;
 constexpr u32 ERR_HASH_OVERFLOW = 4u;       // a bucket chain exceeded BSGS_MAXPROBE
 constexpr u32 ERR_FACTOR_OVERFLOW = 8u;     // factor buffer full (cannot happen: sized to the bitmap)
+constexpr u32 ERR_TMA_TIMEOUT = 16u;        // a bulk copy did not complete within the wait bound
 
 // statistics counters (u64)
 enum Stat {
@@ -71,7 +73,7 @@ struct JobDev {
     u32 *bitmap;         // kcount * words
 };
 
-struct PrimeHdr {        // 72 bytes
+struct PrimeHdr {        // 80 bytes (a 16-byte multiple: copied by TMA bulk copies)
     u64 p;               // 0 = skipped
     u64 q;               // p^-1 mod 2^64
     u64 one;             // 2^64 mod p
@@ -83,7 +85,9 @@ struct PrimeHdr {        // 72 bytes
     u32 smul;            // b^e as an integer when the baby step uses additions, else 0
     u32 pad_;
     u64 Sh;              // Montgomery S^(Lc/2): start of a thread's second giant chain
+    u64 pad2_;
 };
+static_assert(sizeof(PrimeHdr) == 80, "PrimeHdr is copied in 16-byte units");
 
 struct FactorRec {       // one claimed term: p | k[seq]*b^n + c[seq]
     u64 p;

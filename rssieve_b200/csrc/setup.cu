@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
     const u64 p = primes[first + t];
     PrimeHdr H;
     H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.pad_ = 0;
-    H.Sh = 0;
+    H.Sh = 0; H.pad2_ = 0;
     const Mont M = mont_init(p);
     const u32 b = job->base;
     const u64 bm = to_mont(b, M);
