@@ -33,6 +33,11 @@ METRIC = "primes tested/s at 100 seqs, batched vs plain on 1 B200; p50/p99 unit 
 WORKLOAD = ("config2 plain form: 100 seqs k*2^n+-1 (50 +1, 50 -1), k odd U[3,2^32), n in [4e6,1e7) "
             "kept w.p. 0.03, p windows from 2^50")
 P_START = 1 << 50
+# DRAM bytes (read + write) per prime of the BSGS kernel, from one ncu capture
+# of a 2^20-wide window at 2^50 (64.40 MB for 30 243 primes): the 2112-byte
+# prime record plus claims.  Traffic grows in proportion to primes, so the
+# per-launch figure is this times the primes one launch processes.
+BSGS_DRAM_BYTES_PER_PRIME = 2129.4
 
 
 def parse():
@@ -273,7 +278,9 @@ def main():
             "e2e": e2e,
             "gpu_launches": kernel_launches,
             "roofline": {"bound": "int32-imad (64-bit Montgomery products)", "achieved": achieved, "peak": peak,
-                         "unit": "Gmulmod/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "Gmulmod/s", "frac": achieved / peak,
+                         "traffic": BSGS_DRAM_BYTES_PER_PRIME * tot["primes"] / max(bsgs_launches, 1),
+                         "traffic_unit": "bytes per BSGS launch (ncu per-prime DRAM bytes x primes per launch)",
                          "peak_source": "measured live: rs_mulmod_peak, independent Montgomery-product chains"},
             "cpu_baseline": cpu,
             "clocks": clocks,
