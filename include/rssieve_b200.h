@@ -168,6 +168,31 @@ int rs_last_timing(rs_ctx *ctx, double *bsgs_ms, double *total_kernel_ms, uint32
  * integer-multiply-bound BSGS kernel. */
 int rs_mulmod_peak(rs_ctx *ctx, double *gmulmods_per_s, double *ms);
 
+/* Largest range width (p1 - p0) that rs_primes_generate_noalloc accepts. */
+#define RS_NOALLOC_MAX_WIDTH (1ull << 22)
+
+/* The prime generator of rs_primes_generate, for callers that must not
+ * allocate device memory: no cudaMalloc or cudaFree, no allocating library
+ * routine, no context.  No counterpart in the reference (its getsegprimes
+ * writes into buffers that cl_sieve.cpp allocates up front).
+ *
+ * Writes the odd primes of [p0,p1), unordered, to d_primes (caller-owned
+ * device memory, room for cap values) and their total number to *d_count
+ * (caller-owned device word), both on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream).  The call enqueues work and returns; read *d_count
+ * after the stream is done.  If *d_count > cap the output is incomplete:
+ * repeat with more room or a narrower range.  p0 < 3 is raised to 3.
+ *
+ * Scratch is one fixed device array in the library (about 16 MiB per device,
+ * reserved when its module loads).  Hence: p1 - p0 must not exceed
+ * RS_NOALLOC_MAX_WIDTH (RS_EARG otherwise, with the limit in rs_last_error);
+ * the first call on a device does a one-time set-up that waits for `stream`,
+ * so make it before any stream capture; and calls whose work overlaps on one
+ * device (different streams, unordered) race on the shared scratch.  Each call
+ * resets its scratch counters and *d_count itself; nothing needs zeroing. */
+int rs_primes_generate_noalloc(uint64_t p0, uint64_t p1, uint64_t *d_primes, uint32_t cap, uint32_t *d_count,
+                               void *stream);
+
 #ifdef __cplusplus
 }
 #endif

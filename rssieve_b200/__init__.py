@@ -50,8 +50,9 @@ EXPORTS = (
     "rs_factors_file_apply", "rs_factors_commit", "rs_factors_finalize", "rs_state_write", "rs_state_read",
     "rs_state_resume", "rs_ctx_create", "rs_ctx_destroy", "rs_ctx_set_stream", "rs_device_count",
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
-    "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak",
+    "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_primes_generate_noalloc",
 )
+NOALLOC_MAX_WIDTH = 1 << 22     # RS_NOALLOC_MAX_WIDTH
 
 _lib = None
 
@@ -98,6 +99,7 @@ def lib():
         "rs_last_timing": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(u32),
                                      C.POINTER(u32)]),
         "rs_mulmod_peak": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "rs_primes_generate_noalloc": (C.c_int, [u64, u64, vp, u32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

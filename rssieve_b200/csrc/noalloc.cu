@@ -1,0 +1,192 @@
+// noalloc.cu -- prime generation into caller-owned device memory, with no
+// device allocation on any call.
+//
+// The generator behind rs_primes_generate (k_sieve + k_mr of sieve.cu) needs
+// scratch: the table of odd sieving primes below 2^16, the buffer of sieve
+// survivors that k_mr tests, and two counters.  rs_primes_generate keeps
+// these in its context, allocated with cudaMalloc.  This variant keeps them in
+// one file-scope device array of fixed size, g_na_scratch below, so a call
+// allocates nothing; the caller passes the output array and the count word.
+//
+// Limit: a call covers at most RS_NOALLOC_MAX_WIDTH = 2^22 integers, i.e. at
+// most 2^21 odd values, which is exactly the survivor capacity, so the
+// survivor buffer can never overflow.  Wider ranges are rejected with RS_EARG.
+//
+// Set-up: the first call on a device (the device current on the calling
+// thread) looks up the scratch address with cudaGetSymbolAddress, fills the
+// sieving-prime table with a one-CTA kernel on the caller's stream and waits
+// for that stream.  Later calls on the device only enqueue work and return.
+//
+// What starts at zero: every call resets the survivor counter, the error word
+// and the caller's count word with cudaMemsetAsync on the caller's stream
+// before its kernels; the output array needs no clearing.
+//
+// There is one scratch per device: two calls whose work overlaps on the
+// device (different streams, no ordering between them) race on it and give
+// wrong results.  Order them on one stream or with events.
+#include <cstdio>
+#include <mutex>
+
+#include "rs_host.h"
+#include "rs_internal.h"
+
+using namespace rs;
+
+namespace {
+
+constexpr u32 NA_CAND_CAP = 1u << 21;        // survivor slots (u64 each): 16 MiB
+constexpr u32 NA_SP_SLOTS = 6656;            // u32 slots for the 6541 odd primes < 2^16
+constexpr u32 NA_NSP = 6541;                 // pi(2^16) - 1
+constexpr u32 NA_CTR_SLOTS = 64;             // u32: [0] survivors [1] error flags [2] set-up count
+constexpr size_t NA_WORDS = NA_CAND_CAP + NA_SP_SLOTS / 2 + NA_CTR_SLOTS / 2;
+static_assert(RS_NOALLOC_MAX_WIDTH / 2 == NA_CAND_CAP, "survivor capacity must cover every odd value of a call");
+
+// The scratch: survivors, then sieving primes, then counters (all offsets
+// are multiples of 256 bytes).
+static __device__ __align__(256) u64 g_na_scratch[NA_WORDS];
+
+constexpr int NA_MAX_DEVICES = 64;
+struct DevState {
+    u64 *scratch = nullptr;
+    int sms = 0;
+};
+std::mutex g_na_mu;
+DevState g_na_dev[NA_MAX_DEVICES];
+
+// Odd primes below 2^16 in ascending order: one CTA sieves the 2^15 odd
+// values 2i+1 in shared memory and compacts them with a block-wide scan.
+__global__ void __launch_bounds__(1024) k_na_small_primes(u32 *__restrict__ sp, u32 *__restrict__ count)
+{
+    __shared__ u32 comp[1024];                // bit i of word w: value 2(32w+i)+1 is composite
+    __shared__ u32 warp_sum[32];
+    const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    comp[tid] = (tid == 0) ? 1u : 0u;         // 1 is not prime
+    __syncthreads();
+    for (u32 r = 3; r < 256; r += 2) {
+        // multiples r*r, r*r+2r, ... as odd indices (v-1)/2
+        for (u32 i = (r * r - 1) / 2 + tid * r; i < 32768; i += 1024 * r) atomicOr(&comp[i >> 5], 1u << (i & 31));
+    }
+    __syncthreads();
+    const u32 live = ~comp[tid];
+    const u32 cnt = __popc(live);
+    u32 incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        u32 v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= (u32)o) incl += v;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        u32 s = warp_sum[lane], t = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            u32 v = __shfl_up_sync(0xFFFFFFFFu, t, o);
+            if (lane >= (u32)o) t += v;
+        }
+        warp_sum[lane] = t - s;               // exclusive prefix of the warp totals
+        if (lane == 31) *count = t;
+    }
+    __syncthreads();
+    u32 pos = warp_sum[warp] + incl - cnt;
+    u32 bits = live;
+    while (bits) {
+        u32 b = __ffs(bits) - 1;
+        bits &= bits - 1;
+        sp[pos++] = 2 * (tid * 32 + b) + 1;
+    }
+}
+
+#define NA_CU(call)                                                                           \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            rs_set_error("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return RS_ECUDA;                                                                  \
+        }                                                                                     \
+    } while (0)
+
+// Once per device, with that device current: scratch address, SM count and
+// the sieving-prime table.  Waits for the caller's stream.
+int na_setup(int dev, cudaStream_t st, DevState *out)
+{
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_na_scratch);
+    if (e != cudaSuccess || !ptr) {
+        rs_set_error("cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev,
+                     cudaGetErrorString(e));
+        return RS_ECUDA;
+    }
+    int sms = 0;
+    NA_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    u64 *scr = (u64 *)ptr;
+    u32 *sp = (u32 *)(scr + NA_CAND_CAP);
+    u32 *ctrs = sp + NA_SP_SLOTS;
+    k_na_small_primes<<<1, 1024, 0, st>>>(sp, ctrs + 2);
+    NA_CU(cudaGetLastError());
+    u32 n = 0;
+    NA_CU(cudaMemcpyAsync(&n, ctrs + 2, 4, cudaMemcpyDeviceToHost, st));
+    NA_CU(cudaStreamSynchronize(st));
+    if (n != NA_NSP) {
+        rs_set_error("static scratch set-up found %u sieving primes, expected %u", n, NA_NSP);
+        return RS_EDEVICE;
+    }
+    out->scratch = scr;
+    out->sms = sms;
+    return RS_OK;
+}
+
+}  // namespace
+
+extern "C" int rs_primes_generate_noalloc(uint64_t p0, uint64_t p1, uint64_t *d_primes, uint32_t cap,
+                                          uint32_t *d_count, void *stream)
+{
+    if (!d_count || (!d_primes && cap)) {
+        rs_set_error("rs_primes_generate_noalloc: d_count is NULL, or d_primes is NULL with cap > 0");
+        return RS_EARG;
+    }
+    if (p0 >= p1) {
+        rs_set_error("rs_primes_generate_noalloc: empty range [%llu, %llu)", (unsigned long long)p0,
+                     (unsigned long long)p1);
+        return RS_EARG;
+    }
+    if (p1 - p0 > RS_NOALLOC_MAX_WIDTH) {
+        rs_set_error("rs_primes_generate_noalloc: range width %llu exceeds the static scratch limit of %llu "
+                     "integers per call",
+                     (unsigned long long)(p1 - p0), (unsigned long long)RS_NOALLOC_MAX_WIDTH);
+        return RS_EARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        rs_set_error("no CUDA device available");
+        return RS_ENODEV;
+    }
+    int dev = -1;
+    NA_CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NA_MAX_DEVICES) {
+        rs_set_error("device %d is beyond the %d devices this entry point tracks", dev, NA_MAX_DEVICES);
+        return RS_EARG;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    DevState ds;
+    {
+        std::lock_guard<std::mutex> lk(g_na_mu);
+        if (!g_na_dev[dev].scratch) {
+            int rc = na_setup(dev, st, &g_na_dev[dev]);
+            if (rc) return rc;
+        }
+        ds = g_na_dev[dev];
+    }
+    u64 *cands = ds.scratch;
+    u32 *sp = (u32 *)(ds.scratch + NA_CAND_CAP);
+    u32 *ctrs = sp + NA_SP_SLOTS;
+    if (p0 < 3) p0 = 3;
+    u64 base = p0 | 1ull;
+    u64 nodd = (base < p1) ? (p1 - base + 1) / 2 : 0;
+    NA_CU(cudaMemsetAsync(ctrs, 0, 2 * sizeof(u32), st));
+    NA_CU(cudaMemsetAsync(d_count, 0, sizeof(u32), st));
+    if (nodd == 0) return RS_OK;
+    NA_CU(launch_sieve(base, nodd, p1, sp, NA_NSP, cands, NA_CAND_CAP, ctrs, ctrs + 1, st));
+    NA_CU(launch_mr(cands, ctrs, NA_CAND_CAP, (u64 *)d_primes, cap, d_count, ctrs + 1, ds.sms, st));
+    return RS_OK;
+}
