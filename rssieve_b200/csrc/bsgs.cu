@@ -9,99 +9,112 @@
 //                shared-memory hash table.
 //   giant phase  gamma = T_i * S^q for q in [0,M): thread (i,g) walks q in
 //                [g*Lc, (g+1)*Lc) from T_i * S^(g*Lc) as two interleaved
-//                chains, one Montgomery product and one table probe per step
-//                (giant.cl:170-192).  A match
+//                chains, one modular product (Shoup's for p < 2^63, else
+//                Montgomery) and one table probe per step (giant.cl:170-192).  A match
 //                s^j == gamma gives n = nmin + off_i + e*((q+1)*Q - 1 - j).
 //   small order  ord(s) < Q: each target is looked up once and every n in
 //                range with the same residue mod e*ord is claimed (giant.cl:146-168).
 //   claims       atomicAnd on the term's bitmap bit; the first claimer appends
 //                {p, n, seq} to the factor buffer (giant.cl:21-39,158-162).
 //
-// Hash table: NB buckets of four 32-bit slots in shared memory (load 1/2),
-// filled through per-bucket slot counters (see tab_try).
-// A slot holds a 16-bit fingerprint of y, j+1 in bits 1..15 and, in slot 3, an
-// overflow flag in bit 0 that tells a probe to continue into the next bucket
-// (see tab_hash for the bucket and fingerprint).  A fingerprint
-// match is verified exactly by recomputing y_j from its thread's start value,
-// so the search is exact for every 64-bit value (the reference's split
-// lo32/hi32 table cannot find values whose low 32 bits are zero, giant.cl:46,63).
+// Hash table: NB buckets in shared memory.  Bucket b is 16 bytes of
+// fingerprints -- seven 16-bit slots and, in the top half of the last word, a
+// 16-bit count of the values that hashed or spilled into b -- plus seven
+// 16-bit baby indices j in a separate array.  A count above 7 means the bucket
+// overflowed and later values continued into the next bucket (linear probing).
+// A fingerprint match is verified exactly by recomputing y_j from its
+// thread's start value, so the search is exact for every 64-bit value (the
+// reference's split lo32/hi32 table cannot find values whose low 32 bits are
+// zero, giant.cl:46,63).
 #include "mont.cuh"
 #include "rs_internal.h"
+
+#include <type_traits>
 
 namespace rs {
 
 constexpr u32 HMUL = 0x9E3779B1u;
 
 // Table hash of a 64-bit residue: h = (lo32 ^ hi32) * 0x9E3779B1.  The bucket
-// is the top NBLOG bits of h and the 16-bit fingerprint the bits below them.
-// Both words are folded in because the baby chain for small bases is a run of
-// doublings (x -> 2x mod p): the low bits alone repeat shifted patterns and
-// crowd a few buckets.
-template <u32 NBLOG>
-__device__ __forceinline__ void tab_hash(u64 val, u32 &bucket, u32 &key)
+// is floor(h * NB / 2^32), i.e. the top bits of h; the fingerprint comes from
+// the low 16 bits of h with bit 14 cleared and bit 10 set, which makes it the
+// bit pattern of a normal (finite, nonzero) fp16 number.  Both words of the
+// residue are folded in because the baby chain for small bases is a run of
+// doublings whose low bits alone repeat shifted patterns.
+template <u32 NB>
+__device__ __forceinline__ void tab_hash(u64 val, u32 &bucket, u32 &fp)
 {
     const u32 h = ((u32)val ^ (u32)(val >> 32)) * HMUL;
-    bucket = h >> (32 - NBLOG);
-    key = (h << NBLOG) & 0xFFFF0000u;
+    bucket = __umulhi(h, NB);
+    fp = (h & 0xBFFFu) | 0x0400u;
 }
 
-// Slot claim: a 16-bit counter per bucket (two per word) hands out slots with
-// one atomicAdd and no read-before-write.  Slots 0..2 take a plain store; slot
-// 3 takes an atomicOr so a concurrent overflow flag (bit 0) survives.  A value
-// that finds its bucket full flags it and moves to the next bucket.  Returns
-// true when placed; on false, b is the next bucket to try.
-template <u32 NBLOG>
-__device__ __forceinline__ bool tab_try(u32 *tab32, u32 *cnt, u32 &b, u32 ent)
+// Lane-wise fp16 equality of two packed pairs: 0xFFFF per equal half.  For
+// normal fp16 patterns equality of values is equality of bits, and an empty
+// slot (+0) never equals a fingerprint, so this is an exact 16-bit compare
+// that covers two slots per instruction.
+__device__ __forceinline__ u32 heq2(u32 a, u32 b)
 {
-    constexpr u32 NB = 1u << NBLOG;
-    const u32 sh = (b & 1u) << 4;
-    const u32 slot = (atomicAdd(&cnt[b >> 1], 1u << sh) >> sh) & 0xFFFFu;
-    if (slot < 3) { tab32[b * 4 + slot] = ent; return true; }
-    if (slot == 3) { atomicOr(&tab32[b * 4 + 3], ent); return true; }
-    atomicOr(&tab32[b * 4 + 3], 1u);       // bucket full: mark overflow
-    b = (b + 1) & (NB - 1);
+    u32 d;
+    asm("set.eq.u32.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+struct Table {
+    uint4 *fpb;                // NB buckets of fingerprints + count
+    unsigned short *jt;        // j of slot k of bucket b at jt[8*b + k]
+};
+
+// One insertion attempt into bucket b: the count's atomicAdd hands out the
+// slot; slots 0..5 take plain 16-bit stores, slot 6 shares its word with the
+// count and takes an atomicOr.  On a full bucket, b advances and false is
+// returned (the raised count already tells probes to continue).
+template <u32 NB>
+__device__ __forceinline__ bool tab_try(const Table &T, u32 &b, u32 fp, u32 j)
+{
+    u32 *w3 = reinterpret_cast<u32 *>(&T.fpb[b]) + 3;
+    const u32 slot = atomicAdd(w3, 0x10000u) >> 16;
+    if (slot < 6) {
+        reinterpret_cast<unsigned short *>(&T.fpb[b])[slot] = (unsigned short)fp;
+        T.jt[8 * b + slot] = (unsigned short)j;
+        return true;
+    }
+    if (slot == 6) {
+        atomicOr(w3, fp);
+        T.jt[8 * b + 6] = (unsigned short)j;
+        return true;
+    }
+    b = (b + 1 == NB) ? 0u : b + 1;
     return false;
 }
 
-// bit k set when slot k of bucket bv holds an entry whose fingerprint is key
-__device__ __forceinline__ u32 bucket_match(const uint4 &bv, u32 key)
+// halfword k (0..6) of a bucket
+__device__ __forceinline__ u32 slot_fp(const uint4 &bv, int k)
 {
-    u32 m = 0;
-    m |= (((bv.x ^ key) < 0x10000u) & ((bv.x & 0xFFFEu) != 0)) ? 1u : 0u;
-    m |= (((bv.y ^ key) < 0x10000u) & ((bv.y & 0xFFFEu) != 0)) ? 2u : 0u;
-    m |= (((bv.z ^ key) < 0x10000u) & ((bv.z & 0xFFFEu) != 0)) ? 4u : 0u;
-    m |= (((bv.w ^ key) < 0x10000u) & ((bv.w & 0xFFFEu) != 0)) ? 8u : 0u;
-    return m;
-}
-
-__device__ __forceinline__ u32 slot_j(const uint4 &bv, int k)
-{
-    const u32 w = (k == 0) ? bv.x : (k == 1) ? bv.y : (k == 2) ? bv.z : bv.w;
-    return ((w >> 1) & 0x7FFFu) - 1;
+    const u32 w = (k < 2) ? bv.x : (k < 4) ? bv.y : (k < 6) ? bv.z : bv.w;
+    return (k & 1) ? (w >> 16) : (w & 0xFFFFu);
 }
 
 // Calls f(j) for every slot whose fingerprint matches val.  The common case
-// (no match, bucket not flagged) is one 128-bit load, compares and one branch;
-// matches and overflow chains take the out-of-line path.
-template <u32 NBLOG, class F>
-__device__ __forceinline__ void tab_probe(const uint4 *table, u64 val, F &&f)
+// (no match, no overflow) is one 128-bit load, four paired fp16 compares and
+// one branch; matches and overflowed buckets take the out-of-line path.
+template <u32 NB, class F>
+__device__ __forceinline__ void tab_probe(const Table &T, u64 val, F &&f)
 {
-    constexpr u32 NB = 1u << NBLOG;
-    u32 b, key;
-    tab_hash<NBLOG>(val, b, key);
-    uint4 bv = table[b];
-    u32 m = bucket_match(bv, key);
-    if (__builtin_expect((m | (bv.w & 1u)) != 0, 0)) {
+    u32 b, fp;
+    tab_hash<NB>(val, b, fp);
+    const u32 kk = fp * 0x10001u;
+    uint4 bv = T.fpb[b];
+    const u32 m = heq2(bv.x, kk) | heq2(bv.y, kk) | heq2(bv.z, kk) | heq2(bv.w & 0xFFFFu, kk);
+    if (__builtin_expect((m | (bv.w >> 19)) != 0, 0)) {       // bv.w >> 19: count >= 8
         for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
-            while (m) {
-                const int k = __ffs(m) - 1;
-                m &= m - 1;
-                f(slot_j(bv, k));
-            }
-            if (!(bv.w & 1u)) break;
-            b = (b + 1) & (NB - 1);
-            bv = table[b];
-            m = bucket_match(bv, key);
+            const u32 cnt = bv.w >> 16;
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                if ((u32)k < cnt && slot_fp(bv, k) == fp) f((u32)T.jt[8 * b + k]);
+            if (cnt < 8) break;
+            b = (b + 1 == NB) ? 0u : b + 1;
+            bv = T.fpb[b];
         }
     }
 }
@@ -183,19 +196,19 @@ static_assert(sizeof(RecBuf) % 16 == 0, "bulk copies move 16-byte units");
 
 constexpr u32 WAIT_BOUND = 1u << 24;   // try_wait rounds before a copy is declared lost
 
-template <int TPB, int C, int NBLOG>
+template <int TPB, int C, int NB>
 __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__restrict__ hdr,
                                                  const u64 *__restrict__ tabs, const u64 *__restrict__ tgt,
                                                  const unsigned char *__restrict__ meta, u32 count, u32 *work_ctr)
 {
     constexpr u32 Q = TPB * C;
-    constexpr u32 NB = 1u << NBLOG;
+    static_assert(Q <= 65536, "baby indices are stored in 16 bits");
     constexpr int IB = 8;                                         // values inserted per batch
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint4 *table = reinterpret_cast<uint4 *>(smem_raw);
-    u32 *tab32 = reinterpret_cast<u32 *>(table);
-    u32 *s_cnt = reinterpret_cast<u32 *>(table + NB);             // NB 16-bit slot counters
-    u64 *s_start = reinterpret_cast<u64 *>(s_cnt + NB / 2);
+    Table T;
+    T.fpb = reinterpret_cast<uint4 *>(smem_raw);
+    T.jt = reinterpret_cast<unsigned short *>(T.fpb + NB);
+    u64 *s_start = reinterpret_cast<u64 *>(T.jt + 8 * NB);
     u64 *s_Z = s_start + TPB;
     RecBuf *rec = reinterpret_cast<RecBuf *>(s_Z + TPB);          // two staging buffers
     __shared__ __align__(8) u64 s_bar[2];
@@ -252,7 +265,7 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
         const u64 p = R.hdr.p, q = R.hdr.q, s = R.hdr.s;
         const u32 e = R.hdr.e, smul = R.hdr.smul;
         if (live)
-            for (u32 i = tid; i < NB + NB / 8; i += TPB) table[i] = make_uint4(0u, 0u, 0u, 0u);   // table + counters
+            for (u32 i = tid; i < NB; i += TPB) T.fpb[i] = make_uint4(0u, 0u, 0u, 0u);   // fingerprints + counts
         __syncthreads();
         if (s_abort) break;
         if (tid == 0) {
@@ -273,28 +286,30 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
             u32 spill = 0;
 #pragma unroll
             for (int h0 = 0; h0 < C; h0 += IB) {
-                u32 bk[IB], en[IB], old[IB];
+                u32 bk[IB], fp[IB], old[IB];
 #pragma unroll
                 for (int i = 0; i < IB; ++i) {
                     const u32 j = tid * C + h0 + i;
                     if (j != 0 && x == one) atomicMin(&s_order, j);
-                    u32 key;
-                    tab_hash<NBLOG>(x, bk[i], key);
-                    en[i] = key | ((j + 1) << 1);
+                    tab_hash<NB>(x, bk[i], fp[i]);
                     x = baby_step(x, smul, s, p, q);
                 }
 #pragma unroll
-                for (int i = 0; i < IB; ++i) old[i] = atomicAdd(&s_cnt[bk[i] >> 1], 1u << ((bk[i] & 1u) << 4));
+                for (int i = 0; i < IB; ++i) old[i] = atomicAdd(reinterpret_cast<u32 *>(&T.fpb[bk[i]]) + 3, 0x10000u);
 #pragma unroll
                 for (int i = 0; i < IB; ++i) {
-                    const u32 slot = (old[i] >> ((bk[i] & 1u) << 4)) & 0xFFFFu;
-                    if (slot < 3) tab32[bk[i] * 4 + slot] = en[i];
-                    else if (slot == 3) atomicOr(&tab32[bk[i] * 4 + 3], en[i]);
-                    else {
-                        atomicOr(&tab32[bk[i] * 4 + 3], 1u);      // full: flag and try the next buckets
-                        u32 b = (bk[i] + 1) & (NB - 1);
+                    const u32 j = tid * C + h0 + i;
+                    const u32 slot = old[i] >> 16;
+                    if (slot < 6) {
+                        reinterpret_cast<unsigned short *>(&T.fpb[bk[i]])[slot] = (unsigned short)fp[i];
+                        T.jt[8 * bk[i] + slot] = (unsigned short)j;
+                    } else if (slot == 6) {
+                        atomicOr(reinterpret_cast<u32 *>(&T.fpb[bk[i]]) + 3, fp[i]);
+                        T.jt[8 * bk[i] + 6] = (unsigned short)j;
+                    } else {
+                        u32 b = (bk[i] + 1 == NB) ? 0u : bk[i] + 1;   // full: continue in the next buckets
                         int pr = 1;
-                        while (pr < BSGS_SPEC_PROBE && !tab_try<NBLOG>(tab32, s_cnt, b, en[i])) ++pr;
+                        while (pr < BSGS_SPEC_PROBE && !tab_try<NB>(T, b, fp[i], j)) ++pr;
                         if (pr >= BSGS_SPEC_PROBE) spill = 1;
                     }
                 }
@@ -307,17 +322,17 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
         if (live) {
             if (order < Q) {
                 // ord(s) < Q: rebuild the table from the distinct values j < ord
-                for (u32 i = tid; i < NB + NB / 8; i += TPB) table[i] = make_uint4(0u, 0u, 0u, 0u);
+                for (u32 i = tid; i < NB; i += TPB) T.fpb[i] = make_uint4(0u, 0u, 0u, 0u);
                 __syncthreads();
                 u64 y = s_start[tid];
                 u32 pend = 0;
                 for (int i = 0; i < C; ++i) {
                     const u32 j = tid * C + i;
                     if (j < order) {
-                        u32 b, key;
-                        tab_hash<NBLOG>(y, b, key);
+                        u32 b, fpv;
+                        tab_hash<NB>(y, b, fpv);
                         int pr = 0;
-                        while (pr < BSGS_MAXPROBE && !tab_try<NBLOG>(tab32, s_cnt, b, key | ((j + 1) << 1))) ++pr;
+                        while (pr < BSGS_MAXPROBE && !tab_try<NB>(T, b, fpv, j)) ++pr;
                         if (pr >= BSGS_MAXPROBE) pend = 1;
                     }
                     y = baby_step(y, smul, s, p, q);
@@ -339,10 +354,14 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
             if (order == 0xFFFFFFFFu) {
                 // ---- giant steps: two independent chains per thread ----
                 // chain A walks q in [q0, q0+h), chain B q in [q0+h, q1), h = Lc/2;
-                // B starts from A's start times S^h (Sh), so the two Montgomery
-                // products of a step are independent and overlap in the pipeline.
+                // B starts from A's start times S^h (Sh), so the two products of
+                // a step are independent and overlap in the pipeline.  For
+                // p < 2^63 the step is Shoup's product by the fixed s^Q (Sw is its
+                // quotient constant), else the Montgomery product by S; the
+                // choice is uniform over the CTA.
                 const u32 numk = R.hdr.numk, G = R.hdr.G, Lc = R.hdr.Lc;
-                const u64 S = R.hdr.S;
+                const u64 S = R.hdr.S, Sw = R.hdr.Sw;
+                const u64 Sp = from_mont(S, Mont{p, q, 0, 0});
                 if (tid < numk * G) {
                     const u32 i = tid / G, g = tid - i * G;
                     const u32 q0 = g * Lc;
@@ -360,26 +379,31 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
                         const u64 n = (u64)a.nmin + off + (u64)e * u;
                         if (n <= a.nmax) claim(a, p, seq, (u32)n, &s_dups, &s_facs);
                     };
-                    for (u32 t = 0; t < nB; ++t) {
-                        if (t < nA) {
-                            const u32 qa = q0 + t;
-                            const u64 ga = gA;
-                            tab_probe<NBLOG>(table, ga, [&](u32 j) { hit(qa, j, ga); });
-                            gA = mmul(gA, S, p, q);
+                    auto walk = [&](auto shoup) {
+                        constexpr bool SH = decltype(shoup)::value;
+                        for (u32 t = 0; t < nB; ++t) {
+                            if (t < nA) {
+                                const u32 qa = q0 + t;
+                                const u64 ga = gA;
+                                tab_probe<NB>(T, ga, [&](u32 j) { hit(qa, j, ga); });
+                                gA = SH ? shoup_mul(gA, Sp, Sw, p) : mmul(gA, S, p, q);
+                            }
+                            const u32 qb = q0 + h + t;
+                            const u64 gb = gB;
+                            tab_probe<NB>(T, gb, [&](u32 j) { hit(qb, j, gb); });
+                            gB = SH ? shoup_mul(gB, Sp, Sw, p) : mmul(gB, S, p, q);
                         }
-                        const u32 qb = q0 + h + t;
-                        const u64 gb = gB;
-                        tab_probe<NBLOG>(table, gb, [&](u32 j) { hit(qb, j, gb); });
-                        gB = mmul(gB, S, p, q);
-                    }
+                    };
+                    if (Sw) walk(std::true_type{});
+                    else walk(std::false_type{});
                 }
             } else {
                 // ---- ord(s) < Q: one lookup per target ----
                 if (tid < R.hdr.numk) {
-                    const u64 T = R.tgt[tid];
-                    tab_probe<NBLOG>(table, T, [&](u32 j) {
+                    const u64 Tv = R.tgt[tid];
+                    tab_probe<NB>(T, Tv, [&](u32 j) {
                         atomicAdd(&s_cands, 1ull);
-                        if (j >= order || !verify(j, T)) return;
+                        if (j >= order || !verify(j, Tv)) return;
                         const u32 k = atomicAdd(&s_nsol, 1u);
                         s_sol_i[k] = tid;
                         s_sol_u0[k] = (Q - 1 - j) % order;
@@ -427,13 +451,13 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
 
 size_t bsgs_smem_bytes()
 {
-    constexpr size_t NB = 1u << BSGS_NBLOG;
-    return NB * 16 + NB * 2 + BSGS_TPB * 8 * 2 + 2 * sizeof(RecBuf);
+    constexpr size_t NB = BSGS_NB;
+    return NB * 16 + NB * 8 * 2 + BSGS_TPB * 8 * 2 + 2 * sizeof(RecBuf);
 }
 
 cudaError_t bsgs_prepare()
 {
-    return cudaFuncSetAttribute(k_bsgs<BSGS_TPB, BSGS_C, BSGS_NBLOG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)bsgs_smem_bytes());
 }
 
@@ -441,7 +465,7 @@ cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs,
                         const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st)
 {
     if (count == 0) return cudaSuccess;
-    auto kern = k_bsgs<BSGS_TPB, BSGS_C, BSGS_NBLOG>;
+    auto kern = k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB>;
     const size_t smem = bsgs_smem_bytes();
     unsigned grid = ((u32)sms < count) ? (unsigned)sms : (unsigned)count;
     kern<<<grid, BSGS_TPB, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);

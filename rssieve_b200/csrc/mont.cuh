@@ -27,6 +27,31 @@ RS_DEV u64 mmul(u64 a, u64 b, u64 p, u64 q)
     return (hi < mp) ? r + p : r;
 }
 
+// x*w mod p for a fixed multiplier w < p with its precomputed quotient
+// wp = floor(w*2^64/p) (Shoup's method; for p < 2^63).  For any x < 2^64,
+// x*w - floor(x*wp/2^64)*p lies in [0, 2p): one conditional subtraction.
+// Ten 32x32 products against the Montgomery product's eleven, with shorter
+// carry chains.  The representation of x is preserved (x*R times w stays
+// x*w*R), so it mixes freely with Montgomery-form values.
+RS_DEV u64 shoup_mul(u64 x, u64 w, u64 wp, u64 p)
+{
+    const u64 qh = __umul64hi(x, wp);
+    const u64 r = x * w - qh * p;
+    return (r >= p) ? r - p : r;
+}
+
+// floor(w * 2^64 / p) for w < p < 2^63: 64 steps of binary long division.
+RS_DEV u64 shoup_const(u64 w, u64 p)
+{
+    u64 r = w, qt = 0;
+    for (int i = 0; i < 64; ++i) {
+        r <<= 1;                  // r < p < 2^63, so 2r does not wrap
+        qt <<= 1;
+        if (r >= p) { r -= p; qt |= 1; }
+    }
+    return qt;
+}
+
 // a + b mod p for a, b in [0,p); correct for p up to 2^64-1 (wrapping add).
 RS_DEV u64 madd(u64 a, u64 b, u64 p)
 {

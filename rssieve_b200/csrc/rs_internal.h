@@ -23,9 +23,9 @@ constexpr int NDS = 12;              // power-residue degrees of setup.cl:22-48
 constexpr int BSGS_TPB = 1024;
 constexpr int BSGS_C = 16;
 constexpr int BSGS_Q = BSGS_TPB * BSGS_C;   // 16384
-constexpr int BSGS_NBLOG = 13;              // 8192 buckets * 16 B = 128 KiB, load 1/2
+constexpr int BSGS_NB = 6144;               // buckets of 7 slots: 16 B fingerprints + 16 B indices each, load 0.38
 constexpr int BSGS_MAXPROBE = 64;
-constexpr int BSGS_SPEC_PROBE = 64;        // bucket walk bound while ord(s) is still unknown (walks of 17 occur about once per 10^4 primes)
+constexpr int BSGS_SPEC_PROBE = 64;         // bucket walk bound while ord(s) is still unknown
 
 constexpr int SETUP_TPB = 256;              // 8 primes (warps) per block
 constexpr int SIEVE_TPB = 512;
@@ -85,7 +85,7 @@ struct PrimeHdr {        // 80 bytes (a 16-byte multiple: copied by TMA bulk cop
     u32 smul;            // b^e as an integer when the baby step uses additions, else 0
     u32 pad_;
     u64 Sh;              // Montgomery S^(Lc/2): start of a thread's second giant chain
-    u64 pad2_;
+    u64 Sw;              // floor(Sp*2^64/p), Sp = s^Q mod p (plain), for Shoup giant steps; 0 when p >= 2^63
 };
 static_assert(sizeof(PrimeHdr) == 80, "PrimeHdr is copied in 16-byte units");
 

@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
     const u64 p = primes[first + t];
     PrimeHdr H;
     H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.pad_ = 0;
-    H.Sh = 0; H.pad2_ = 0;
+    H.Sh = 0; H.Sw = 0;
     const Mont M = mont_init(p);
     const u32 b = job->base;
     const u64 bm = to_mont(b, M);
@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
     for (int w = 0; w < 32; ++w) { tb[32 + w] = a; a = mmul(a, v, p, M.q); }
     const u64 bb = (e == 2) ? (u64)b * b : (u64)b;
     H.p = p; H.q = M.q; H.one = M.one; H.s = s; H.S = S; H.e = e;
+    H.Sw = (p >> 63) ? 0 : shoup_const(from_mont(S, M), p);   // nonzero: from_mont(S) = s^Q != 0 mod p
     H.smul = (bb <= 16) ? (u32)bb : 0u;
     hdr[t] = H;
     aux[t] = X;
