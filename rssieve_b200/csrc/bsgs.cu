@@ -18,10 +18,11 @@
 //                {p, n, seq} to the factor buffer (giant.cl:21-39,158-162).
 //
 // Hash table: NB buckets in shared memory.  Bucket b is 16 bytes of
-// fingerprints -- seven 16-bit slots and, in the top half of the last word, a
-// 16-bit count of the values that hashed or spilled into b -- plus seven
-// 16-bit baby indices j in a separate array.  A count above 7 means the bucket
-// overflowed and later values continued into the next bucket (linear probing).
+// fingerprints -- seven 16-bit slots and, in bit 31 of the last word, an
+// overflow flag meaning that later values continued into the next bucket
+// (linear probing) -- plus seven 16-bit baby indices j in a separate array and
+// a 16-bit fill count in a third (two per word, so that the counts' atomics
+// spread over all shared-memory banks).
 // A fingerprint match is verified exactly by recomputing y_j from its
 // thread's start value, so the search is exact for every 64-bit value (the
 // reference's split lo32/hi32 table cannot find values whose low 32 bits are
@@ -61,19 +62,26 @@ __device__ __forceinline__ u32 heq2(u32 a, u32 b)
 }
 
 struct Table {
-    uint4 *fpb;                // NB buckets of fingerprints + count
+    uint4 *fpb;                // NB buckets of fingerprints + overflow flag
     unsigned short *jt;        // j of slot k of bucket b at jt[8*b + k]
+    u32 *cnt;                  // fill count of bucket b in half (b & 1) of cnt[b >> 1]
 };
 
-// One insertion attempt into bucket b: the count's atomicAdd hands out the
-// slot; slots 0..5 take plain 16-bit stores, slot 6 shares its word with the
-// count and takes an atomicOr.  On a full bucket, b advances and false is
-// returned (the raised count already tells probes to continue).
-template <u32 NB>
-__device__ __forceinline__ bool tab_try(const Table &T, u32 &b, u32 fp, u32 j)
+constexpr u32 OVF_FLAG = 0x80000000u;   // bit 31 of a bucket's last word
+
+// Slot claim in bucket b: the count's atomicAdd hands out the slot.
+__device__ __forceinline__ u32 tab_claim(const Table &T, u32 b)
+{
+    const u32 sh = (b & 1u) << 4;
+    return (atomicAdd(&T.cnt[b >> 1], 1u << sh) >> sh) & 0xFFFFu;
+}
+
+// Fills slot `slot` of bucket b, or flags b as overflowed when slot > 6.
+// Slots 0..5 take plain 16-bit stores; slot 6 shares its word with the flag
+// and takes an atomicOr.  Returns whether the value was placed.
+__device__ __forceinline__ bool tab_fill(const Table &T, u32 b, u32 slot, u32 fp, u32 j)
 {
     u32 *w3 = reinterpret_cast<u32 *>(&T.fpb[b]) + 3;
-    const u32 slot = atomicAdd(w3, 0x10000u) >> 16;
     if (slot < 6) {
         reinterpret_cast<unsigned short *>(&T.fpb[b])[slot] = (unsigned short)fp;
         T.jt[8 * b + slot] = (unsigned short)j;
@@ -84,6 +92,16 @@ __device__ __forceinline__ bool tab_try(const Table &T, u32 &b, u32 fp, u32 j)
         T.jt[8 * b + 6] = (unsigned short)j;
         return true;
     }
+    atomicOr(w3, OVF_FLAG);
+    return false;
+}
+
+// One insertion attempt into bucket b; on a full bucket, b advances and false
+// is returned.
+template <u32 NB>
+__device__ __forceinline__ bool tab_try(const Table &T, u32 &b, u32 fp, u32 j)
+{
+    if (tab_fill(T, b, tab_claim(T, b), fp, j)) return true;
     b = (b + 1 == NB) ? 0u : b + 1;
     return false;
 }
@@ -95,30 +113,6 @@ __device__ __forceinline__ u32 slot_fp(const uint4 &bv, int k)
     return (k & 1) ? (w >> 16) : (w & 0xFFFFu);
 }
 
-// Calls f(j) for every slot whose fingerprint matches val.  The common case
-// (no match, no overflow) is one 128-bit load, four paired fp16 compares and
-// one branch; matches and overflowed buckets take the out-of-line path.
-template <u32 NB, class F>
-__device__ __forceinline__ void tab_probe(const Table &T, u64 val, F &&f)
-{
-    u32 b, fp;
-    tab_hash<NB>(val, b, fp);
-    const u32 kk = fp * 0x10001u;
-    uint4 bv = T.fpb[b];
-    const u32 m = heq2(bv.x, kk) | heq2(bv.y, kk) | heq2(bv.z, kk) | heq2(bv.w & 0xFFFFu, kk);
-    if (__builtin_expect((m | (bv.w >> 19)) != 0, 0)) {       // bv.w >> 19: count >= 8
-        for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
-            const u32 cnt = bv.w >> 16;
-#pragma unroll
-            for (int k = 0; k < 7; ++k)
-                if ((u32)k < cnt && slot_fp(bv, k) == fp) f((u32)T.jt[8 * b + k]);
-            if (cnt < 8) break;
-            b = (b + 1 == NB) ? 0u : b + 1;
-            bv = T.fpb[b];
-        }
-    }
-}
-
 // y -> y*s: doubling/quadrupling for b = 2 (the common case), additions for
 // b^e <= 16, a Montgomery product otherwise (smul is uniform per prime)
 __device__ __forceinline__ u64 baby_step(u64 x, u32 smul, u64 s, u64 p, u64 q)
@@ -126,28 +120,6 @@ __device__ __forceinline__ u64 baby_step(u64 x, u32 smul, u64 s, u64 p, u64 q)
     if (smul == 2) return madd(x, x, p);
     if (smul == 4) { x = madd(x, x, p); return madd(x, x, p); }
     return smul ? mul_small(x, smul, p) : mmul(x, s, p, q);
-}
-
-__device__ __forceinline__ void claim(const BsgsArgs &a, u64 p, u32 seq, u32 n, unsigned long long *s_dups,
-                                      unsigned long long *s_facs)
-{
-    const u32 o = n - a.nmin;
-    u32 *w = a.bitmap + (size_t)seq * a.words + (o >> 5);
-    const u32 mask = 1u << (o & 31);
-    const u32 old = atomicAnd(w, ~mask);
-    if (old & mask) {
-        const u32 f = atomicAdd(a.factor_ctr, 1u);
-        atomicAdd(s_facs, 1ull);
-        if (f < a.factor_cap) {
-            FactorRec r;
-            r.p = p; r.n = n; r.seq = seq;
-            a.factors[f] = r;
-        } else {
-            atomicOr(a.err, ERR_FACTOR_OVERFLOW);
-        }
-    } else {
-        atomicAdd(s_dups, 1ull);
-    }
 }
 
 // ---- TMA 1D bulk copies and mbarriers (record prefetch) ----
@@ -196,7 +168,202 @@ static_assert(sizeof(RecBuf) % 16 == 0, "bulk copies move 16-byte units");
 
 constexpr u32 WAIT_BOUND = 1u << 24;   // try_wait rounds before a copy is declared lost
 
+// ---- per-CTA state in shared memory, read by the out-of-line rare paths ----
+// The hot loops stay small (and in the instruction cache) because matches,
+// overflowed buckets, small orders and claims run in __noinline__ functions
+// that take a few scalars and find everything else here.
+struct PrimeCtx {
+    u64 p, q, s;         // the prime, -p^-1 mod 2^64, Montgomery b^e
+    u32 smul, e;         // baby-step multiplier when additions suffice; 1 or 2
+};
+extern __shared__ __align__(128) unsigned char smem_raw[];
+__shared__ BsgsArgs s_args;
+__shared__ PrimeCtx s_ctx;
+__shared__ unsigned long long s_cands, s_dups, s_facs;   // per-CTA totals
+__shared__ u32 s_nsol, s_sol_i[KMAX], s_sol_u0[KMAX];   // small-order solutions
+
+// Dynamic shared memory: fingerprints | indices | counts | start values | giant
+// start powers | two record staging buffers.
+template <int TPB, int NB>
+struct Smem {
+    static __device__ __forceinline__ Table table()
+    {
+        Table T;
+        T.fpb = reinterpret_cast<uint4 *>(smem_raw);
+        T.jt = reinterpret_cast<unsigned short *>(T.fpb + NB);
+        T.cnt = reinterpret_cast<u32 *>(T.jt + 8 * NB);
+        return T;
+    }
+    static __device__ __forceinline__ u64 *start() { return reinterpret_cast<u64 *>(table().cnt + NB / 2); }
+    static __device__ __forceinline__ u64 *zs() { return start() + TPB; }
+    static __device__ __forceinline__ RecBuf *rec() { return reinterpret_cast<RecBuf *>(zs() + TPB); }
+    static constexpr size_t bytes() { return (size_t)NB * 16 + (size_t)NB * 16 + (size_t)NB * 2 + (size_t)TPB * 16 + 2 * sizeof(RecBuf); }
+};
+
+// First claimer of term (seq, n) clears its bitmap bit and appends the factor.
+__device__ __forceinline__ void claim(u64 p, u32 seq, u32 n)
+{
+    const BsgsArgs &a = s_args;
+    const u32 o = n - a.nmin;
+    u32 *w = a.bitmap + (size_t)seq * a.words + (o >> 5);
+    const u32 mask = 1u << (o & 31);
+    const u32 old = atomicAnd(w, ~mask);
+    if (old & mask) {
+        const u32 f = atomicAdd(a.factor_ctr, 1u);
+        atomicAdd(&s_facs, 1ull);
+        if (f < a.factor_cap) {
+            FactorRec r;
+            r.p = p; r.n = n; r.seq = seq;
+            a.factors[f] = r;
+        } else {
+            atomicOr(a.err, ERR_FACTOR_OVERFLOW);
+        }
+    } else {
+        atomicAdd(&s_dups, 1ull);
+    }
+}
+
+// exact check of a fingerprint match: y_j == val ?  (y_j from its thread's start)
+template <int C>
+__device__ __forceinline__ bool verify(const u64 *s_start, u32 j, u64 val, u32 Q)
+{
+    if (j >= Q) return false;
+    const PrimeCtx c = s_ctx;
+    u64 y = s_start[j / C];
+    for (u32 r = j % C; r; --r) y = baby_step(y, c.smul, c.s, c.p, c.q);
+    return y == val;
+}
+
+// Giant-step match or overflowed bucket: check every matching slot of the
+// chain starting at bucket b exactly and claim n = nmin + off + e*((q+1)Q-1-j).
 template <int TPB, int C, int NB>
+__device__ __noinline__ void giant_slow(u64 gamma, u32 b, u32 fp, u32 qq, u32 meta)
+{
+    constexpr u32 Q = TPB * C;
+    const Table T = Smem<TPB, NB>::table();
+    const u64 *st = Smem<TPB, NB>::start();
+    for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
+        const uint4 bv = T.fpb[b];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            if (slot_fp(bv, k) != fp) continue;
+            atomicAdd(&s_cands, 1ull);
+            const u32 j = T.jt[8 * b + k];
+            if (!verify<C>(st, j, gamma, Q)) continue;
+            const u64 u = (u64)(qq + 1) * Q - 1 - j;
+            const u64 n = (u64)s_args.nmin + (meta >> 7) + (u64)s_ctx.e * u;
+            if (n <= s_args.nmax) claim(s_ctx.p, meta & 0x7Fu, (u32)n);
+        }
+        if (!(bv.w & OVF_FLAG)) break;
+        b = (b + 1 == NB) ? 0u : b + 1;
+    }
+}
+
+// The giant step's table probe: one 128-bit load, four paired fp16 compares
+// and one branch in the common case.  The flag half of the last word (0 or
+// 0x8000, i.e. +-0 as fp16) never equals a fingerprint, so all eight halves
+// are compared without masking.
+template <int TPB, int C, int NB>
+__device__ __forceinline__ void giant_probe(const Table &T, u64 g, u32 qq, u32 meta)
+{
+    u32 b, fp;
+    tab_hash<NB>(g, b, fp);
+    const u32 kk = fp * 0x10001u;
+    const uint4 bv = T.fpb[b];
+    const u32 m = heq2(bv.x, kk) | heq2(bv.y, kk) | heq2(bv.z, kk) | heq2(bv.w, kk);
+    if (__builtin_expect((m | (bv.w & OVF_FLAG)) != 0, 0)) giant_slow<TPB, C, NB>(g, b, fp, qq, meta);
+}
+
+// Continues an insertion whose home bucket was full; returns 1 if the walk
+// gave up after maxprobe buckets.
+template <int NB>
+__device__ __noinline__ u32 insert_walk(u32 b, u32 fp, u32 j, int maxprobe)
+{
+    const Table T = Smem<0, NB>::table();
+    b = (b + 1 == NB) ? 0u : b + 1;
+    for (int pr = 1; pr < maxprobe; ++pr)
+        if (tab_try<NB>(T, b, fp, j)) return 0;
+    return 1;
+}
+
+__device__ __forceinline__ void clear_table(const Table &T, u32 nb)
+{
+    for (u32 i = threadIdx.x; i < nb; i += blockDim.x) T.fpb[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (u32 i = threadIdx.x; i < nb / 8; i += blockDim.x) reinterpret_cast<uint4 *>(T.cnt)[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+// ord(s) < Q: rebuild the table from the distinct values j < ord (the
+// speculative one may hold repeats).  Called by the whole CTA.
+template <int TPB, int C, int NB>
+__device__ __noinline__ void rebuild_table(u32 order)
+{
+    const Table T = Smem<TPB, NB>::table();
+    const u64 *st = Smem<TPB, NB>::start();
+    const PrimeCtx c = s_ctx;
+    clear_table(T, NB);
+    __syncthreads();
+    u64 y = st[threadIdx.x];
+    u32 pend = 0;
+    for (int i = 0; i < C; ++i) {
+        const u32 j = threadIdx.x * C + i;
+        if (j < order) {
+            u32 b, fpv;
+            tab_hash<NB>(y, b, fpv);
+            int pr = 0;
+            while (pr < BSGS_MAXPROBE && !tab_try<NB>(T, b, fpv, j)) ++pr;
+            if (pr >= BSGS_MAXPROBE) pend = 1;
+        }
+        y = baby_step(y, c.smul, c.s, c.p, c.q);
+    }
+    if (pend) atomicOr(s_args.err, ERR_HASH_OVERFLOW);
+    __syncthreads();
+}
+
+// ord(s) < Q: each target is looked up once; every n in range with the same
+// residue mod e*ord is claimed (giant.cl:146-168).  Called by the whole CTA.
+template <int TPB, int C, int NB>
+__device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
+{
+    constexpr u32 Q = TPB * C;
+    const Table T = Smem<TPB, NB>::table();
+    const u64 *st = Smem<TPB, NB>::start();
+    const u32 tid = threadIdx.x;
+    if (tid < R->hdr.numk) {
+        const u64 Tv = R->tgt[tid];
+        u32 b, fp;
+        tab_hash<NB>(Tv, b, fp);
+        for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
+            const uint4 bv = T.fpb[b];
+            for (int k = 0; k < 7; ++k) {
+                if (slot_fp(bv, k) != fp) continue;
+                atomicAdd(&s_cands, 1ull);
+                const u32 j = T.jt[8 * b + k];
+                if (j >= order || !verify<C>(st, j, Tv, Q)) continue;
+                const u32 ks = atomicAdd(&s_nsol, 1u);
+                s_sol_i[ks] = tid;
+                s_sol_u0[ks] = (Q - 1 - j) % order;
+            }
+            if (!(bv.w & OVF_FLAG)) break;
+            b = (b + 1 == NB) ? 0u : b + 1;
+        }
+    }
+    __syncthreads();
+    const u32 nsol = s_nsol;
+    const u32 e = s_ctx.e;
+    for (u32 k = 0; k < nsol; ++k) {
+        const u32 m = R->meta[s_sol_i[k]];
+        const u32 seq = m & 0x7Fu, off = m >> 7;
+        for (u64 u = s_sol_u0[k] + (u64)tid * order;; u += (u64)TPB * order) {
+            const u64 n = (u64)s_args.nmin + off + (u64)e * u;
+            if (n > s_args.nmax) break;
+            claim(s_ctx.p, seq, (u32)n);
+        }
+    }
+}
+
+// MODE: 1 = every prime below 2^63 (Shoup giant steps), 0 = every prime at or
+// above 2^63 (Montgomery giant steps), 2 = mixed, chosen per prime.
+template <int TPB, int C, int NB, int MODE>
 __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__restrict__ hdr,
                                                  const u64 *__restrict__ tabs, const u64 *__restrict__ tgt,
                                                  const unsigned char *__restrict__ meta, u32 count, u32 *work_ctr)
@@ -204,17 +371,12 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
     constexpr u32 Q = TPB * C;
     static_assert(Q <= 65536, "baby indices are stored in 16 bits");
     constexpr int IB = 8;                                         // values inserted per batch
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    Table T;
-    T.fpb = reinterpret_cast<uint4 *>(smem_raw);
-    T.jt = reinterpret_cast<unsigned short *>(T.fpb + NB);
-    u64 *s_start = reinterpret_cast<u64 *>(T.jt + 8 * NB);
-    u64 *s_Z = s_start + TPB;
-    RecBuf *rec = reinterpret_cast<RecBuf *>(s_Z + TPB);          // two staging buffers
+    const Table T = Smem<TPB, NB>::table();
+    u64 *s_start = Smem<TPB, NB>::start();
+    u64 *s_Z = Smem<TPB, NB>::zs();
+    RecBuf *rec = Smem<TPB, NB>::rec();                           // two staging buffers
     __shared__ __align__(8) u64 s_bar[2];
-    __shared__ unsigned long long s_cands, s_dups, s_facs;        // per-kernel totals
-    __shared__ u32 s_idx[2], s_order, s_nsol, s_spill, s_abort;
-    __shared__ u32 s_sol_i[KMAX], s_sol_u0[KMAX];
+    __shared__ u32 s_idx[2], s_order, s_spill, s_abort;
 
     const u32 tid = threadIdx.x;
     auto fetch = [&](u32 buf, u32 idx) {                          // thread 0 only
@@ -230,6 +392,7 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_args = a;
         s_abort = 0;
         s_cands = 0;
         s_dups = 0;
@@ -251,6 +414,10 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
                 if (++n > WAIT_BOUND) { atomicOr(&s_abort, 1u); break; }
             }
         }
+        const RecBuf &R = rec[buf];
+        const bool live = (R.hdr.p != 0);
+        const u64 p = R.hdr.p, q = R.hdr.q, s = R.hdr.s;
+        const u32 e = R.hdr.e, smul = R.hdr.smul;
         // claim the next prime; the result is consumed after the table clear,
         // so this warp keeps issuing while the atomic is in flight
         u32 nxt = 0;
@@ -258,14 +425,10 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
             s_order = 0xFFFFFFFFu;
             s_nsol = 0;
             s_spill = 0;
+            s_ctx.p = p; s_ctx.q = q; s_ctx.s = s; s_ctx.smul = smul; s_ctx.e = e;
             nxt = atomicAdd(work_ctr, 1u);
         }
-        const RecBuf &R = rec[buf];
-        const bool live = (R.hdr.p != 0);
-        const u64 p = R.hdr.p, q = R.hdr.q, s = R.hdr.s;
-        const u32 e = R.hdr.e, smul = R.hdr.smul;
-        if (live)
-            for (u32 i = tid; i < NB; i += TPB) T.fpb[i] = make_uint4(0u, 0u, 0u, 0u);   // fingerprints + counts
+        if (live) clear_table(T, NB);
         __syncthreads();
         if (s_abort) break;
         if (tid == 0) {
@@ -279,7 +442,7 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
             if (tid < R.hdr.G) s_Z[tid] = mmul(R.tabs[64 + (tid & 31)], R.tabs[96 + (tid >> 5)], p, q);
             // ---- baby steps y_j = s^j, inserted as they are produced ----
             // Speculative: ord(s) < Q is only known after the barrier; then the
-            // table (which may hold repeats) is rebuilt from j < ord below.
+            // table (which may hold repeats) is rebuilt from j < ord.
             const u64 one = R.hdr.one;
             u64 x = mmul(R.tabs[tid & 31], R.tabs[32 + (tid >> 5)], p, q);   // s^(C*tid)
             s_start[tid] = x;
@@ -295,23 +458,11 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
                     x = baby_step(x, smul, s, p, q);
                 }
 #pragma unroll
-                for (int i = 0; i < IB; ++i) old[i] = atomicAdd(reinterpret_cast<u32 *>(&T.fpb[bk[i]]) + 3, 0x10000u);
+                for (int i = 0; i < IB; ++i) old[i] = tab_claim(T, bk[i]);
 #pragma unroll
                 for (int i = 0; i < IB; ++i) {
                     const u32 j = tid * C + h0 + i;
-                    const u32 slot = old[i] >> 16;
-                    if (slot < 6) {
-                        reinterpret_cast<unsigned short *>(&T.fpb[bk[i]])[slot] = (unsigned short)fp[i];
-                        T.jt[8 * bk[i] + slot] = (unsigned short)j;
-                    } else if (slot == 6) {
-                        atomicOr(reinterpret_cast<u32 *>(&T.fpb[bk[i]]) + 3, fp[i]);
-                        T.jt[8 * bk[i] + 6] = (unsigned short)j;
-                    } else {
-                        u32 b = (bk[i] + 1 == NB) ? 0u : bk[i] + 1;   // full: continue in the next buckets
-                        int pr = 1;
-                        while (pr < BSGS_SPEC_PROBE && !tab_try<NB>(T, b, fp[i], j)) ++pr;
-                        if (pr >= BSGS_SPEC_PROBE) spill = 1;
-                    }
+                    if (!tab_fill(T, bk[i], old[i], fp[i], j)) spill |= insert_walk<NB>(bk[i], fp[i], j, BSGS_SPEC_PROBE);
                 }
             }
             if (spill) s_spill = 1;
@@ -320,45 +471,16 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
         const u32 order = s_order;
         const u32 Mg = (e == 2) ? a.M2 : a.M1;
         if (live) {
-            if (order < Q) {
-                // ord(s) < Q: rebuild the table from the distinct values j < ord
-                for (u32 i = tid; i < NB; i += TPB) T.fpb[i] = make_uint4(0u, 0u, 0u, 0u);
-                __syncthreads();
-                u64 y = s_start[tid];
-                u32 pend = 0;
-                for (int i = 0; i < C; ++i) {
-                    const u32 j = tid * C + i;
-                    if (j < order) {
-                        u32 b, fpv;
-                        tab_hash<NB>(y, b, fpv);
-                        int pr = 0;
-                        while (pr < BSGS_MAXPROBE && !tab_try<NB>(T, b, fpv, j)) ++pr;
-                        if (pr >= BSGS_MAXPROBE) pend = 1;
-                    }
-                    y = baby_step(y, smul, s, p, q);
-                }
-                if (pend) atomicOr(a.err, ERR_HASH_OVERFLOW);
-                __syncthreads();
-            } else if (tid == 0 && s_spill) {
-                atomicOr(a.err, ERR_HASH_OVERFLOW);
-            }
-
-            // exact check of a fingerprint match: y_j == val ?
-            auto verify = [&](u32 j, u64 val) -> bool {
-                if (j >= Q) return false;
-                u64 y = s_start[j / C];
-                for (u32 r = j % C; r; --r) y = baby_step(y, smul, s, p, q);
-                return y == val;
-            };
+            if (order < Q) rebuild_table<TPB, C, NB>(order);
+            else if (tid == 0 && s_spill) atomicOr(a.err, ERR_HASH_OVERFLOW);
 
             if (order == 0xFFFFFFFFu) {
                 // ---- giant steps: two independent chains per thread ----
                 // chain A walks q in [q0, q0+h), chain B q in [q0+h, q1), h = Lc/2;
                 // B starts from A's start times S^h (Sh), so the two products of
-                // a step are independent and overlap in the pipeline.  For
-                // p < 2^63 the step is Shoup's product by the fixed s^Q (Sw is its
-                // quotient constant), else the Montgomery product by S; the
-                // choice is uniform over the CTA.
+                // a step are independent and overlap in the pipeline.  Below
+                // 2^63 the step is Shoup's product by the fixed s^Q (Sw is its
+                // quotient constant), else the Montgomery product by S.
                 const u32 numk = R.hdr.numk, G = R.hdr.G, Lc = R.hdr.Lc;
                 const u64 S = R.hdr.S, Sw = R.hdr.Sw;
                 const u64 Sp = from_mont(S, Mont{p, q, 0, 0});
@@ -369,58 +491,26 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
                     const u32 h = Lc >> 1;
                     const u32 nA = min(h, q1 - q0), nB = (q1 - q0) - nA;
                     const u32 m = R.meta[i];
-                    const u32 seq = m & 0x7Fu, off = m >> 7;
                     u64 gA = mmul(R.tgt[i], s_Z[g], p, q);
                     u64 gB = mmul(gA, R.hdr.Sh, p, q);
-                    auto hit = [&](u32 qq, u32 j, u64 gamma) {
-                        atomicAdd(&s_cands, 1ull);
-                        if (!verify(j, gamma)) return;
-                        const u64 u = (u64)(qq + 1) * Q - 1 - j;
-                        const u64 n = (u64)a.nmin + off + (u64)e * u;
-                        if (n <= a.nmax) claim(a, p, seq, (u32)n, &s_dups, &s_facs);
-                    };
                     auto walk = [&](auto shoup) {
                         constexpr bool SH = decltype(shoup)::value;
                         for (u32 t = 0; t < nB; ++t) {
                             if (t < nA) {
-                                const u32 qa = q0 + t;
-                                const u64 ga = gA;
-                                tab_probe<NB>(T, ga, [&](u32 j) { hit(qa, j, ga); });
+                                giant_probe<TPB, C, NB>(T, gA, q0 + t, m);
                                 gA = SH ? shoup_mul(gA, Sp, Sw, p) : mmul(gA, S, p, q);
                             }
-                            const u32 qb = q0 + h + t;
-                            const u64 gb = gB;
-                            tab_probe<NB>(T, gb, [&](u32 j) { hit(qb, j, gb); });
+                            giant_probe<TPB, C, NB>(T, gB, q0 + h + t, m);
                             gB = SH ? shoup_mul(gB, Sp, Sw, p) : mmul(gB, S, p, q);
                         }
                     };
-                    if (Sw) walk(std::true_type{});
+                    if (MODE == 1) walk(std::true_type{});
+                    else if (MODE == 0) walk(std::false_type{});
+                    else if (Sw) walk(std::true_type{});
                     else walk(std::false_type{});
                 }
             } else {
-                // ---- ord(s) < Q: one lookup per target ----
-                if (tid < R.hdr.numk) {
-                    const u64 Tv = R.tgt[tid];
-                    tab_probe<NB>(T, Tv, [&](u32 j) {
-                        atomicAdd(&s_cands, 1ull);
-                        if (j >= order || !verify(j, Tv)) return;
-                        const u32 k = atomicAdd(&s_nsol, 1u);
-                        s_sol_i[k] = tid;
-                        s_sol_u0[k] = (Q - 1 - j) % order;
-                    });
-                }
-                __syncthreads();
-                const u32 nsol = s_nsol;
-                for (u32 k = 0; k < nsol; ++k) {
-                    const u32 i = s_sol_i[k];
-                    const u32 m = R.meta[i];
-                    const u32 seq = m & 0x7Fu, off = m >> 7;
-                    for (u64 u = s_sol_u0[k] + (u64)tid * order;; u += (u64)TPB * order) {
-                        const u64 n = (u64)a.nmin + off + (u64)e * u;
-                        if (n > a.nmax) break;
-                        claim(a, p, seq, (u32)n, &s_dups, &s_facs);
-                    }
-                }
+                small_order_search<TPB, C, NB>(&R, order);
             }
             if (tid == 0) {
                 st_baby += min(order, Q);
@@ -449,26 +539,39 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
     }
 }
 
-size_t bsgs_smem_bytes()
+using BsgsSmem = Smem<BSGS_TPB, BSGS_NB>;
+
+size_t bsgs_smem_bytes() { return BsgsSmem::bytes(); }
+
+template <int MODE>
+static cudaError_t set_smem()
 {
-    constexpr size_t NB = BSGS_NB;
-    return NB * 16 + NB * 8 * 2 + BSGS_TPB * 8 * 2 + 2 * sizeof(RecBuf);
+    return cudaFuncSetAttribute(k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bsgs_smem_bytes());
 }
 
 cudaError_t bsgs_prepare()
 {
-    return cudaFuncSetAttribute(k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)bsgs_smem_bytes());
+    cudaError_t e = set_smem<0>();
+    if (e == cudaSuccess) e = set_smem<1>();
+    if (e == cudaSuccess) e = set_smem<2>();
+    return e;
 }
 
 cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
-                        const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st)
+                        const unsigned char *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int sms,
+                        cudaStream_t st)
 {
     if (count == 0) return cudaSuccess;
-    auto kern = k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB>;
     const size_t smem = bsgs_smem_bytes();
-    unsigned grid = ((u32)sms < count) ? (unsigned)sms : (unsigned)count;
-    kern<<<grid, BSGS_TPB, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
+    const unsigned grid = ((u32)sms < count) ? (unsigned)sms : (unsigned)count;
+    const u64 TOP = 1ull << 63;
+    if (pmax <= TOP)
+        k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB, 1><<<grid, BSGS_TPB, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
+    else if (pmin >= TOP)
+        k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB, 0><<<grid, BSGS_TPB, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
+    else
+        k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB, 2><<<grid, BSGS_TPB, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
     return cudaGetLastError();
 }
 

@@ -387,7 +387,7 @@ extern "C" int rs_run_range(rs_ctx *c, uint64_t p0, uint64_t p1, rs_counters *de
                             c->d_stats, c->stream));
             CU(cudaMemsetAsync(c->d_ctrs + 2, 0, 4, c->stream));
             CU(cudaEventRecord(c->ev[2 + 2 * ci], c->stream));
-            CU(launch_bsgs(a, c->d_hdr, c->d_tabs, c->d_tgt, c->d_meta, cnt, c->d_ctrs + 2, c->sms, c->stream));
+            CU(launch_bsgs(a, c->d_hdr, c->d_tabs, c->d_tgt, c->d_meta, cnt, c->d_ctrs + 2, p, hi, c->sms, c->stream));
             CU(cudaEventRecord(c->ev[3 + 2 * ci], c->stream));
             c->last_kernel_launches += 3;
             c->last_bsgs_launches += 1;

@@ -23,7 +23,7 @@ constexpr int NDS = 12;              // power-residue degrees of setup.cl:22-48
 constexpr int BSGS_TPB = 1024;
 constexpr int BSGS_C = 16;
 constexpr int BSGS_Q = BSGS_TPB * BSGS_C;   // 16384
-constexpr int BSGS_NB = 6144;               // buckets of 7 slots: 16 B fingerprints + 16 B indices each, load 0.38
+constexpr int BSGS_NB = 6144;               // buckets of 7 slots: 16 B fingerprints + 16 B indices + 2 B count, load 0.38
 constexpr int BSGS_MAXPROBE = 64;
 constexpr int BSGS_SPEC_PROBE = 64;         // bucket walk bound while ord(s) is still unknown
 
@@ -115,7 +115,8 @@ cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 co
                          u64 *tgt, unsigned char *meta, u64 *stats, cudaStream_t st);
 size_t setup_aux_bytes();
 cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
-                        const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st);
+                        const unsigned char *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int sms,
+                        cudaStream_t st);   // every prime of the launch lies in [pmin, pmax)
 size_t bsgs_smem_bytes();
 cudaError_t bsgs_prepare();   // per device, before the first launch
 cudaError_t launch_mulmod_peak(u64 *out, int blocks, int iters, cudaStream_t st);
