@@ -18,11 +18,12 @@
 //                {p, n, seq} to the factor buffer (giant.cl:21-39,158-162).
 //
 // Hash table: NB buckets in shared memory.  Bucket b is 16 bytes of
-// fingerprints -- seven 16-bit slots and, in bit 31 of the last word, an
-// overflow flag meaning that later values continued into the next bucket
+// fingerprints -- seven 16-bit slots and an eighth halfword that is 0x8000
+// when the bucket overflowed, i.e. later values continued into the next bucket
 // (linear probing) -- plus seven 16-bit baby indices j in a separate array and
 // a 16-bit fill count in a third (two per word, so that the counts' atomics
-// spread over all shared-memory banks).
+// spread over all shared-memory banks).  Every halfword has one writer or
+// writers of one value, so all table writes are plain 16-bit stores.
 // A fingerprint match is verified exactly by recomputing y_j from its
 // thread's start value, so the search is exact for every 64-bit value (the
 // reference's split lo32/hi32 table cannot find values whose low 32 bits are
@@ -67,7 +68,7 @@ struct Table {
     u32 *cnt;                  // fill count of bucket b in half (b & 1) of cnt[b >> 1]
 };
 
-constexpr u32 OVF_FLAG = 0x80000000u;   // bit 31 of a bucket's last word
+constexpr u32 OVF_FLAG = 0x80000000u;   // bit 31 of a bucket's last word: halfword 7 = 0x8000
 
 // Slot claim in bucket b: the count's atomicAdd hands out the slot.
 __device__ __forceinline__ u32 tab_claim(const Table &T, u32 b)
@@ -77,22 +78,16 @@ __device__ __forceinline__ u32 tab_claim(const Table &T, u32 b)
 }
 
 // Fills slot `slot` of bucket b, or flags b as overflowed when slot > 6.
-// Slots 0..5 take plain 16-bit stores; slot 6 shares its word with the flag
-// and takes an atomicOr.  Returns whether the value was placed.
+// Returns whether the value was placed.
 __device__ __forceinline__ bool tab_fill(const Table &T, u32 b, u32 slot, u32 fp, u32 j)
 {
-    u32 *w3 = reinterpret_cast<u32 *>(&T.fpb[b]) + 3;
-    if (slot < 6) {
-        reinterpret_cast<unsigned short *>(&T.fpb[b])[slot] = (unsigned short)fp;
+    unsigned short *h = reinterpret_cast<unsigned short *>(&T.fpb[b]);
+    if (slot < 7) {
+        h[slot] = (unsigned short)fp;
         T.jt[8 * b + slot] = (unsigned short)j;
         return true;
     }
-    if (slot == 6) {
-        atomicOr(w3, fp);
-        T.jt[8 * b + 6] = (unsigned short)j;
-        return true;
-    }
-    atomicOr(w3, OVF_FLAG);
+    h[7] = 0x8000u;
     return false;
 }
 
@@ -271,7 +266,16 @@ __device__ __forceinline__ void giant_probe(const Table &T, u64 g, u32 qq, u32 m
     const u32 kk = fp * 0x10001u;
     const uint4 bv = T.fpb[b];
     const u32 m = heq2(bv.x, kk) | heq2(bv.y, kk) | heq2(bv.z, kk) | heq2(bv.w, kk);
-    if (__builtin_expect((m | (bv.w & OVF_FLAG)) != 0, 0)) giant_slow<TPB, C, NB>(g, b, fp, qq, meta);
+    if (__builtin_expect((m | (bv.w & OVF_FLAG)) != 0, 0)) {
+        // about 1% of buckets overflowed: with no match here, the next bucket
+        // is checked inline, and only matches or longer chains go out of line
+        bool slow = (m != 0);
+        if (!slow) {
+            const uint4 bn = T.fpb[(b + 1 == NB) ? 0u : b + 1];
+            slow = ((heq2(bn.x, kk) | heq2(bn.y, kk) | heq2(bn.z, kk) | heq2(bn.w, kk)) | (bn.w & OVF_FLAG)) != 0;
+        }
+        if (slow) giant_slow<TPB, C, NB>(g, b, fp, qq, meta);
+    }
 }
 
 // Continues an insertion whose home bucket was full; returns 1 if the walk
