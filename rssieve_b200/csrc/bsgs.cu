@@ -499,13 +499,18 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
                     u64 gB = mmul(gA, R.hdr.Sh, p, q);
                     auto walk = [&](auto shoup) {
                         constexpr bool SH = decltype(shoup)::value;
-                        for (u32 t = 0; t < nB; ++t) {
+                        // chain B has nA or nA+1 steps, except in a target's last,
+                        // shorter chunk, where it may have fewer or none
+                        const u32 nt = max(nA, nB);
+                        for (u32 t = 0; t < nt; ++t) {
                             if (t < nA) {
                                 giant_probe<TPB, C, NB>(T, gA, q0 + t, m);
                                 gA = SH ? shoup_mul(gA, Sp, Sw, p) : mmul(gA, S, p, q);
                             }
-                            giant_probe<TPB, C, NB>(T, gB, q0 + h + t, m);
-                            gB = SH ? shoup_mul(gB, Sp, Sw, p) : mmul(gB, S, p, q);
+                            if (t < nB) {
+                                giant_probe<TPB, C, NB>(T, gB, q0 + h + t, m);
+                                gB = SH ? shoup_mul(gB, Sp, Sw, p) : mmul(gB, S, p, q);
+                            }
                         }
                     };
                     if (MODE == 1) walk(std::true_type{});

@@ -78,3 +78,13 @@ def test_large_k_near_2_64(sieve, oracle, rs):
     job = W.small_job(24, kcount=20, base=5, nmin=1000, nmax=200000, keep=0.05, kmax=1 << 40)
     lo = (1 << 64) - (1 << 22)
     _check_job(sieve, oracle, job, lo, (1 << 64) - 1, rs)
+
+
+@pytest.mark.parametrize("seed,kcount,base", [(31, 100, 2), (32, 12, 2), (33, 40, 3), (34, 24, 7)])
+def test_long_n_range_many_giant_chunks(sieve, oracle, rs, seed, kcount, base):
+    """n-range of 4*10^6: hundreds of giant steps per target, split into chunks
+    whose last one is shorter (a second chain that is empty or one step short),
+    against the brute-force oracle over a window with thousands of factors.
+    Bases 3 and 7 take the general baby step (b^e added or multiplied)."""
+    job = W.small_job(seed, kcount=kcount, base=base, nmin=1_000_000, nmax=4_999_999, keep=0.05, kmax=1 << 28)
+    _check_job(sieve, oracle, job, 3_000_000, 3_004_000, rs)
