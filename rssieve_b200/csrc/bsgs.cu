@@ -110,6 +110,13 @@ __device__ __forceinline__ u32 slot_fp(const uint4 &bv, int k)
 
 // y -> y*s: doubling/quadrupling for b = 2 (the common case), additions for
 // b^e <= 16, a Montgomery product otherwise (smul is uniform per prime)
+// 2x mod p for p < 2^63 (2x cannot wrap): one compare, one predicated subtract
+__device__ __forceinline__ u64 dbl63(u64 x, u64 p)
+{
+    x += x;
+    return (x >= p) ? x - p : x;
+}
+
 __device__ __forceinline__ u64 baby_step(u64 x, u32 smul, u64 s, u64 p, u64 q)
 {
     if (smul == 2) return madd(x, x, p);
@@ -451,24 +458,37 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
             u64 x = mmul(R.tabs[tid & 31], R.tabs[32 + (tid >> 5)], p, q);   // s^(C*tid)
             s_start[tid] = x;
             u32 spill = 0;
+            // The step kind is uniform per prime (b^e = 2, 4 or other) and is
+            // chosen once, so the loop body carries no dispatch; the first j > 0
+            // with y_j = 1 is kept per thread and merged with one atomicMin.
+            u32 minj = 0xFFFFFFFFu;
+            auto babies = [&](auto kind) {
+                constexpr int K = decltype(kind)::value;          // b^e = 2 or 4 (doublings), else 0
 #pragma unroll
-            for (int h0 = 0; h0 < C; h0 += IB) {
-                u32 bk[IB], fp[IB], old[IB];
+                for (int h0 = 0; h0 < C; h0 += IB) {
+                    u32 bk[IB], fp[IB], old[IB];
 #pragma unroll
-                for (int i = 0; i < IB; ++i) {
-                    const u32 j = tid * C + h0 + i;
-                    if (j != 0 && x == one) atomicMin(&s_order, j);
-                    tab_hash<NB>(x, bk[i], fp[i]);
-                    x = baby_step(x, smul, s, p, q);
+                    for (int i = 0; i < IB; ++i) {
+                        const u32 j = tid * C + h0 + i;
+                        if (j != 0 && x == one && minj == 0xFFFFFFFFu) minj = j;
+                        tab_hash<NB>(x, bk[i], fp[i]);
+                        if (K == 0) x = baby_step(x, smul, s, p, q);
+                        else if (MODE == 1) { x = dbl63(x, p); if (K == 4) x = dbl63(x, p); }
+                        else { x = madd(x, x, p); if (K == 4) x = madd(x, x, p); }
+                    }
+#pragma unroll
+                    for (int i = 0; i < IB; ++i) old[i] = tab_claim(T, bk[i]);
+#pragma unroll
+                    for (int i = 0; i < IB; ++i) {
+                        const u32 j = tid * C + h0 + i;
+                        if (!tab_fill(T, bk[i], old[i], fp[i], j)) spill |= insert_walk<NB>(bk[i], fp[i], j, BSGS_SPEC_PROBE);
+                    }
                 }
-#pragma unroll
-                for (int i = 0; i < IB; ++i) old[i] = tab_claim(T, bk[i]);
-#pragma unroll
-                for (int i = 0; i < IB; ++i) {
-                    const u32 j = tid * C + h0 + i;
-                    if (!tab_fill(T, bk[i], old[i], fp[i], j)) spill |= insert_walk<NB>(bk[i], fp[i], j, BSGS_SPEC_PROBE);
-                }
-            }
+            };
+            if (smul == 2) babies(std::integral_constant<int, 2>{});
+            else if (smul == 4) babies(std::integral_constant<int, 4>{});
+            else babies(std::integral_constant<int, 0>{});
+            if (minj != 0xFFFFFFFFu) atomicMin(&s_order, minj);
             if (spill) s_spill = 1;
         }
         __syncthreads();
