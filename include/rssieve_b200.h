@@ -143,6 +143,16 @@ void rs_ctx_destroy(rs_ctx *ctx);
 int rs_ctx_set_stream(rs_ctx *ctx, void *stream);
 int rs_device_count(void);
 
+/* Baby steps per prime Q for the BSGS search of this context's jobs: 1024,
+ * 2048, 4096, 8192 or 16384, or 0 (the default) to choose per job.  Replaces
+ * the reference's Q/M rule, which fixes Q from the n-range when the kernels
+ * are built (cl_sieve.cpp:893-938).  In automatic mode a model of the per-prime
+ * cost keeps the candidates within 2x of its best, the first full chunks of
+ * the job run with each in turn (their results count, as every Q is exact),
+ * and the fastest measured one is kept.  Takes effect at once. */
+int rs_set_baby_steps(rs_ctx *ctx, uint32_t q);
+/* The Q in use; *tuning (may be NULL) is 1 while candidates are being timed. */
+int rs_get_baby_steps(rs_ctx *ctx, uint32_t *q, int *tuning);
 /* Upload a job: sequences, n-range and bitmap (cl_sieve.cpp:1115-1120,1266). */
 int rs_job_load(rs_ctx *ctx, const rs_seqs *s);
 /* Sieve every prime in [p0,p1) (3 <= p0 < p1 <= 2^64-1): one pass of the

@@ -51,7 +51,9 @@ EXPORTS = (
     "rs_state_resume", "rs_ctx_create", "rs_ctx_destroy", "rs_ctx_set_stream", "rs_device_count",
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
     "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_primes_generate_noalloc",
+    "rs_set_baby_steps", "rs_get_baby_steps",
 )
+BABY_STEPS = (1024, 2048, 4096, 8192, 16384)   # accepted by rs_set_baby_steps (0: automatic)
 NOALLOC_MAX_WIDTH = 1 << 22     # RS_NOALLOC_MAX_WIDTH
 
 _lib = None
@@ -100,6 +102,8 @@ def lib():
                                      C.POINTER(u32)]),
         "rs_mulmod_peak": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "rs_primes_generate_noalloc": (C.c_int, [u64, u64, vp, u32, vp, vp]),
+        "rs_set_baby_steps": (C.c_int, [vp, u32]),
+        "rs_get_baby_steps": (C.c_int, [vp, C.POINTER(u32), C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -312,6 +316,16 @@ class Sieve:
         out = np.zeros(max(cap, 1), dtype=np.uint64)
         _check(L.rs_primes_generate(self._c, p0, p1, out.ctypes.data, cap, C.byref(n)), "rs_primes_generate")
         return out[: n.value].copy()
+
+    def set_baby_steps(self, q):
+        """Force Q baby steps per prime (one of BABY_STEPS), or 0 to choose per job."""
+        _check(lib().rs_set_baby_steps(self._c, q), "rs_set_baby_steps")
+
+    def baby_steps(self):
+        """(Q in use, whether the per-job tuner is still timing candidates)."""
+        q, t = C.c_uint32(0), C.c_int(0)
+        _check(lib().rs_get_baby_steps(self._c, C.byref(q), C.byref(t)), "rs_get_baby_steps")
+        return q.value, bool(t.value)
 
     def mulmod_peak(self):
         """10^9 Montgomery products/s of independent chains on this device."""

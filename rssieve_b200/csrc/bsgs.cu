@@ -373,9 +373,10 @@ __device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
 }
 
 // MODE: 1 = every prime below 2^63 (Shoup giant steps), 0 = every prime at or
-// above 2^63 (Montgomery giant steps), 2 = mixed, chosen per prime.
+// above 2^63 (Montgomery giant steps).  1024 / TPB CTAs share an SM, so the
+// bound keeps each thread at 64 registers.
 template <int TPB, int C, int NB, int MODE>
-__global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__restrict__ hdr,
+__global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const PrimeHdr *__restrict__ hdr,
                                                  const u64 *__restrict__ tabs, const u64 *__restrict__ tgt,
                                                  const unsigned char *__restrict__ meta, u32 count, u32 *work_ctr)
 {
@@ -534,8 +535,6 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
                         }
                     };
                     if (MODE == 1) walk(std::true_type{});
-                    else if (MODE == 0) walk(std::false_type{});
-                    else if (Sw) walk(std::true_type{});
                     else walk(std::false_type{});
                 }
             } else {
@@ -568,40 +567,83 @@ __global__ void __launch_bounds__(TPB, 1) k_bsgs(BsgsArgs a, const PrimeHdr *__r
     }
 }
 
-using BsgsSmem = Smem<BSGS_TPB, BSGS_NB>;
+template <int G, int MODE>
+static cudaError_t launch_geom(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
+                              const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st)
+{
+    constexpr BsgsGeom g = BSGS_GEOMS[G];
+    auto kern = k_bsgs<g.tpb, g.c, g.nb, MODE>;
+    const size_t smem = Smem<g.tpb, g.nb>::bytes();
+    static thread_local int per_sm[32] = {0};            // resident CTAs per SM, per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int &occ = per_sm[dev & 31];
+    if (occ == 0) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, g.tpb, smem);
+        if (e != cudaSuccess) return e;
+        if (occ < 1) return cudaErrorInvalidConfiguration;
+    }
+    const u64 want = (u64)sms * (u64)occ;
+    const unsigned grid = (unsigned)((want < count) ? want : count);
+    kern<<<grid, g.tpb, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
+    return cudaGetLastError();
+}
 
-size_t bsgs_smem_bytes() { return BsgsSmem::bytes(); }
-
-template <int MODE>
+template <int G, int MODE>
 static cudaError_t set_smem()
 {
-    return cudaFuncSetAttribute(k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)bsgs_smem_bytes());
+    constexpr BsgsGeom g = BSGS_GEOMS[G];
+    return cudaFuncSetAttribute(k_bsgs<g.tpb, g.c, g.nb, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)Smem<g.tpb, g.nb>::bytes());
+}
+
+template <int G>
+static size_t smem_of() { return Smem<BSGS_GEOMS[G].tpb, BSGS_GEOMS[G].nb>::bytes(); }
+
+size_t bsgs_smem_bytes(int geom)
+{
+    switch (geom) {
+    case 0: return smem_of<0>();
+    case 1: return smem_of<1>();
+    case 2: return smem_of<2>();
+    case 3: return smem_of<3>();
+    default: return smem_of<4>();
+    }
 }
 
 cudaError_t bsgs_prepare()
 {
-    cudaError_t e = set_smem<0>();
-    if (e == cudaSuccess) e = set_smem<1>();
-    if (e == cudaSuccess) e = set_smem<2>();
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    chk(set_smem<0, 0>()); chk(set_smem<0, 1>());
+    chk(set_smem<1, 0>()); chk(set_smem<1, 1>());
+    chk(set_smem<2, 0>()); chk(set_smem<2, 1>());
+    chk(set_smem<3, 0>()); chk(set_smem<3, 1>());
+    chk(set_smem<4, 0>()); chk(set_smem<4, 1>());
     return e;
 }
 
 cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
-                        const unsigned char *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int sms,
+                        const unsigned char *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int geom, int sms,
                         cudaStream_t st)
 {
     if (count == 0) return cudaSuccess;
-    const size_t smem = bsgs_smem_bytes();
-    const unsigned grid = ((u32)sms < count) ? (unsigned)sms : (unsigned)count;
     const u64 TOP = 1ull << 63;
-    if (pmax <= TOP)
-        k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB, 1><<<grid, BSGS_TPB, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
-    else if (pmin >= TOP)
-        k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB, 0><<<grid, BSGS_TPB, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
-    else
-        k_bsgs<BSGS_TPB, BSGS_C, BSGS_NB, 2><<<grid, BSGS_TPB, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
-    return cudaGetLastError();
+    if (pmin < TOP && pmax > TOP) return cudaErrorInvalidValue;   // the caller splits launches at 2^63
+    const bool shoup = (pmax <= TOP);
+#define RS_BSGS_CASE(G)                                                                                  \
+    case G:                                                                                              \
+        return shoup ? launch_geom<G, 1>(a, hdr, tabs, tgt, meta, count, work_ctr, sms, st)              \
+                     : launch_geom<G, 0>(a, hdr, tabs, tgt, meta, count, work_ctr, sms, st);
+    switch (geom) {
+        RS_BSGS_CASE(0)
+        RS_BSGS_CASE(1)
+        RS_BSGS_CASE(2)
+        RS_BSGS_CASE(3)
+        RS_BSGS_CASE(4)
+    default: return cudaErrorInvalidValue;
+    }
+#undef RS_BSGS_CASE
 }
 
 }  // namespace rs

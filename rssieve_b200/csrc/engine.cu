@@ -49,6 +49,15 @@ struct rs_ctx {
     FactorRec *d_factors = nullptr;
     u32 factor_cap = 0;
     u64 primes_total = 0;
+    // BSGS geometry: forced (index into BSGS_GEOMS) or chosen per job by the tuner
+    int geom_forced = -1;
+    int geom = 0;
+    bool tuning = false;
+    int tune_cand[NGEOM];
+    int tune_ncand = 0, tune_next = 0;
+    double tune_ms[NGEOM];
+    u64 tune_primes[NGEOM];
+    std::vector<int> chunk_geom;
     // timing of the last rs_run_range
     std::vector<cudaEvent_t> ev;
     double last_bsgs_ms = 0, last_total_ms = 0;
@@ -163,7 +172,7 @@ extern "C" int rs_ctx_create(int device, rs_ctx **out)
         cudaMemset(c->d_stats, 0, ST_COUNT * 8) != cudaSuccess)
         return fail(RS_ECUDA);
     if (bsgs_prepare() != cudaSuccess) {
-        rs_set_error("BSGS kernel needs %zu B of shared memory", bsgs_smem_bytes());
+        rs_set_error("BSGS kernel needs %zu B of shared memory", bsgs_smem_bytes(0));
         return fail(RS_ECUDA);
     }
     (void)rc;
@@ -185,6 +194,80 @@ static void odd_split(u64 x, u64 &odd, u32 &v2)
     odd = x;
 }
 
+// Model cost of one prime for a geometry, in baby-step units: Q baby steps plus
+// the giant steps of the targets that survive the prefilter (about 0.6 of the
+// sequences; half the primes use the parity split, which halves their range),
+// a giant step costing about 1.2 baby steps, and the per-prime fixed work
+// (table clear, barriers) of about 0.15 Q.
+static double geom_model_cost(int g, u32 kcount, u32 L)
+{
+    const double q = BSGS_GEOMS[g].q;
+    const double giant = 0.6 * kcount * 0.75 * std::ceil((double)L / q);
+    return 1.15 * q + 1.2 * giant;
+}
+
+// Starts the per-job tuner: the candidates are the geometries whose model cost
+// is within 2x of the model's best; the first chunks cycle through them.
+static void tune_start(rs_ctx *c)
+{
+    c->tune_ncand = 0;
+    c->tune_next = 0;
+    for (int g = 0; g < NGEOM; ++g) { c->tune_ms[g] = 0; c->tune_primes[g] = 0; }
+    if (c->geom_forced >= 0) {
+        c->geom = c->geom_forced;
+        c->tuning = false;
+        return;
+    }
+    double best = 1e300;
+    int gb = 0;
+    for (int g = 0; g < NGEOM; ++g) {
+        double v = geom_model_cost(g, c->h_job.kcount, c->h_job.L);
+        if (v < best) { best = v; gb = g; }
+    }
+    for (int g = 0; g < NGEOM; ++g)
+        if (geom_model_cost(g, c->h_job.kcount, c->h_job.L) <= 2.0 * best) c->tune_cand[c->tune_ncand++] = g;
+    c->geom = gb;
+    c->tuning = (c->tune_ncand > 1);
+}
+
+// Records one chunk's BSGS time; ends tuning once every candidate has timed at
+// least 2^18 primes, keeping the fastest per prime.
+static void tune_record(rs_ctx *c, int g, u32 primes, float ms)
+{
+    if (!c->tuning || primes < 32768) return;
+    c->tune_ms[g] += ms;
+    c->tune_primes[g] += primes;
+    for (int i = 0; i < c->tune_ncand; ++i)
+        if (c->tune_primes[c->tune_cand[i]] < (1u << 18)) return;
+    double best = 1e300;
+    for (int i = 0; i < c->tune_ncand; ++i) {
+        const int gi = c->tune_cand[i];
+        const double v = c->tune_ms[gi] / (double)c->tune_primes[gi];
+        if (v < best) { best = v; c->geom = gi; }
+    }
+    c->tuning = false;
+}
+
+extern "C" int rs_set_baby_steps(rs_ctx *c, uint32_t q)
+{
+    if (!c) return RS_EARG;
+    if (q != 0 && geom_index(q) < 0) {
+        rs_set_error("baby-step count %u is not one of 1024, 2048, 4096, 8192, 16384 (or 0 for automatic)", q);
+        return RS_EARG;
+    }
+    c->geom_forced = q ? geom_index(q) : -1;
+    if (c->job_loaded) tune_start(c);
+    return RS_OK;
+}
+
+extern "C" int rs_get_baby_steps(rs_ctx *c, uint32_t *q, int *tuning)
+{
+    if (!c || !q) return RS_EARG;
+    *q = BSGS_GEOMS[c->geom].q;
+    if (tuning) *tuning = c->tuning ? 1 : 0;
+    return RS_OK;
+}
+
 extern "C" int rs_job_load(rs_ctx *c, const rs_seqs *s)
 {
     if (!c || !s) return RS_EARG;
@@ -200,8 +283,6 @@ extern "C" int rs_job_load(rs_ctx *c, const rs_seqs *s)
     J.nmax = s->nmax;
     J.L = s->nmax - s->nmin + 1;
     J.words = (u32)s->words_per_seq;
-    J.M1 = (u32)((J.L + (u64)BSGS_Q - 1) / BSGS_Q);
-    J.M2 = (u32)((J.L + 2ull * BSGS_Q - 1) / (2ull * BSGS_Q));
     for (u32 i = 0; i < s->kcount; ++i) {
         J.k[i] = s->k[i];
         J.c[i] = s->c[i];
@@ -229,6 +310,7 @@ extern "C" int rs_job_load(rs_ctx *c, const rs_seqs *s)
     CU(cudaStreamSynchronize(c->stream));
     c->primes_total = 0;
     c->job_loaded = true;
+    tune_start(c);
     return RS_OK;
 }
 
@@ -347,8 +429,6 @@ extern "C" int rs_run_range(rs_ctx *c, uint64_t p0, uint64_t p1, rs_counters *de
     a.nmin = c->h_job.nmin;
     a.nmax = c->h_job.nmax;
     a.words = c->h_job.words;
-    a.M1 = c->h_job.M1;
-    a.M2 = c->h_job.M2;
     a.bitmap = c->d_bitmap;
     a.factors = c->d_factors;
     a.factor_ctr = c->d_ctrs + 3;
@@ -358,8 +438,10 @@ extern "C" int rs_run_range(rs_ctx *c, uint64_t p0, uint64_t p1, rs_counters *de
     u64 p = p0;
     u64 width = segment_width(c, p);
     u64 seg_primes = 0;
+    const u64 TOP = 1ull << 63;
     while (p < p1) {
         u64 hi = (p1 - p > width) ? p + width : p1;
+        if (p < TOP && hi > TOP) hi = TOP;          // a launch is either all Shoup or all Montgomery
         rc = ensure_events(c, 2);
         if (rc) return rc;
         CU(cudaEventRecord(c->ev[0], c->stream));
@@ -380,14 +462,22 @@ extern "C" int rs_run_range(rs_ctx *c, uint64_t p0, uint64_t p1, rs_counters *de
         rc = ensure_events(c, 2 + 2 * (size_t)nchunks);
         if (rc) return rc;
         CU(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
+        c->chunk_geom.assign(nchunks, c->geom);
         for (u32 ci = 0; ci < nchunks; ++ci) {
             u32 first = ci * c->chunk_cap;
             u32 cnt = std::min(c->chunk_cap, np - first);
+            // while tuning, full chunks cycle through the candidate geometries
+            const int g = (c->tuning && cnt >= 32768) ? c->tune_cand[c->tune_next++ % c->tune_ncand] : c->geom;
+            c->chunk_geom[ci] = g;
+            const u32 Q = BSGS_GEOMS[g].q;
+            a.M1 = (u32)(((u64)c->h_job.L + Q - 1) / Q);
+            a.M2 = (u32)(((u64)c->h_job.L + 2ull * Q - 1) / (2ull * Q));
             CU(launch_setup(c->d_job, c->d_primes, first, cnt, c->d_hdr, c->d_aux, c->d_tabs, c->d_tgt, c->d_meta,
-                            c->d_stats, c->stream));
+                            c->d_stats, g, c->h_job.L, c->stream));
             CU(cudaMemsetAsync(c->d_ctrs + 2, 0, 4, c->stream));
             CU(cudaEventRecord(c->ev[2 + 2 * ci], c->stream));
-            CU(launch_bsgs(a, c->d_hdr, c->d_tabs, c->d_tgt, c->d_meta, cnt, c->d_ctrs + 2, p, hi, c->sms, c->stream));
+            CU(launch_bsgs(a, c->d_hdr, c->d_tabs, c->d_tgt, c->d_meta, cnt, c->d_ctrs + 2, p, hi, g, c->sms,
+                           c->stream));
             CU(cudaEventRecord(c->ev[3 + 2 * ci], c->stream));
             c->last_kernel_launches += 3;
             c->last_bsgs_launches += 1;
@@ -406,6 +496,7 @@ extern "C" int rs_run_range(rs_ctx *c, uint64_t p0, uint64_t p1, rs_counters *de
         for (u32 ci = 0; ci < nchunks; ++ci) {
             CU(cudaEventElapsedTime(&ms, c->ev[2 + 2 * ci], c->ev[3 + 2 * ci]));
             c->last_bsgs_ms += ms;
+            tune_record(c, c->chunk_geom[ci], std::min(c->chunk_cap, np - ci * c->chunk_cap), ms);
         }
         seg_primes += np;
         p = hi;

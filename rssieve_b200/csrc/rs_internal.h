@@ -19,11 +19,24 @@ constexpr int KSTRIDE = 112;         // padded per-prime target stride (16-byte 
 constexpr int TABS = 128;            // u64 power-table entries per prime
 constexpr int NDS = 12;              // power-residue degrees of setup.cl:22-48
 
-// BSGS kernel shape: Q = BSGS_TPB * BSGS_C baby steps, NB buckets of 4 slots.
-constexpr int BSGS_TPB = 1024;
-constexpr int BSGS_C = 16;
-constexpr int BSGS_Q = BSGS_TPB * BSGS_C;   // 16384
-constexpr int BSGS_NB = 6144;               // buckets of 7 slots: 16 B fingerprints + 16 B indices + 2 B count, load 0.38
+// BSGS kernel geometries: Q = tpb * c baby steps per prime, nb buckets of
+// seven slots (load about 0.4), 1024 / tpb CTAs per SM sharing its 228 KB of
+// shared memory.  The giant phase needs tpb >= KMAX (one thread per target).
+struct BsgsGeom {
+    u32 q, tpb, c, nb;
+};
+constexpr int NGEOM = 5;
+constexpr BsgsGeom BSGS_GEOMS[NGEOM] = {
+    {16384, 1024, 16, 6144},   // 1 CTA per SM
+    {8192, 512, 16, 2944},     // 2
+    {4096, 256, 16, 1408},     // 4
+    {2048, 256, 8, 704},       // 4
+    {1024, 128, 8, 352},       // 8
+};
+constexpr int geom_index(u32 q)
+{
+    return q == 16384 ? 0 : q == 8192 ? 1 : q == 4096 ? 2 : q == 2048 ? 3 : q == 1024 ? 4 : -1;
+}
 constexpr int BSGS_MAXPROBE = 64;
 constexpr int BSGS_SPEC_PROBE = 64;         // bucket walk bound while ord(s) is still unknown
 
@@ -61,7 +74,6 @@ struct JobDev {
     u32 base, kcount, nmin, nmax;
     u32 L;               // nmax - nmin + 1
     u32 words;           // bitmap words per sequence
-    u32 M1, M2;          // giant steps: ceil(L/Q) full, ceil(L/(2Q)) parity
     u64 k[KMAX];
     int c[KMAX];
     u64 kodd[KMAX];      // odd part of k_i
@@ -97,7 +109,7 @@ struct FactorRec {       // one claimed term: p | k[seq]*b^n + c[seq]
 
 struct BsgsArgs {
     u32 base, nmin, nmax, words;
-    u32 M1, M2;
+    u32 M1, M2;          // giant steps per target for this launch's Q: ceil(L/Q), ceil(L/(2Q))
     u32 *bitmap;
     FactorRec *factors;
     u32 *factor_ctr;
@@ -112,12 +124,13 @@ cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp,
 cudaError_t launch_mr(const u64 *cands, const u32 *ctrs, u32 cand_cap, u64 *primes, u32 prime_cap, u32 *prime_ctr,
                       u32 *err, int sms, cudaStream_t st);
 cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 count, PrimeHdr *hdr, void *aux, u64 *tabs,
-                         u64 *tgt, unsigned char *meta, u64 *stats, cudaStream_t st);
+                         u64 *tgt, unsigned char *meta, u64 *stats, int geom, u32 L, cudaStream_t st);
 size_t setup_aux_bytes();
+// every prime of the launch lies in [pmin, pmax), entirely below or entirely at or above 2^63
 cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
-                        const unsigned char *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int sms,
-                        cudaStream_t st);   // every prime of the launch lies in [pmin, pmax)
-size_t bsgs_smem_bytes();
+                        const unsigned char *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int geom, int sms,
+                        cudaStream_t st);
+size_t bsgs_smem_bytes(int geom);
 cudaError_t bsgs_prepare();   // per device, before the first launch
 cudaError_t launch_mulmod_peak(u64 *out, int blocks, int iters, cudaStream_t st);
 

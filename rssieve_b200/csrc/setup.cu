@@ -62,9 +62,15 @@ struct PrimeAux {        // kernel 1 -> kernel 2 scalars
     u32 pad_;
 };
 
+// The BSGS geometry of a launch: Q = tpb * c baby steps, and the giant steps
+// per target that Q implies.
+struct SetupGeom {
+    u32 q, c, tpb, m1, m2;
+};
+
 __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ job, const u64 *__restrict__ primes,
                                                      u32 first, u32 count, PrimeHdr *__restrict__ hdr,
-                                                     PrimeAux *__restrict__ aux, u64 *__restrict__ tabs)
+                                                     PrimeAux *__restrict__ aux, u64 *__restrict__ tabs, SetupGeom gm)
 {
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
@@ -79,8 +85,8 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
     const int rg = legendre_of(job->bodd, job->bv2, job->brd, p);
     const u32 e = (rg == -1) ? 2u : 1u;
     const u64 s = (e == 2) ? mmul(bm, bm, p, M.q) : bm;
-    const u64 S = mpow(s, (u64)BSGS_Q, M);
-    const u64 W0 = mpow(bm, (u64)job->nmin + (u64)e * (BSGS_Q - 1), M);
+    const u64 S = mpow(s, (u64)gm.q, M);
+    const u64 W0 = mpow(bm, (u64)job->nmin + (u64)e * (gm.q - 1), M);
     PrimeAux X;
     X.r2 = M.r2;
     X.wr0 = mmul(W0, M.r2, p, M.q);
@@ -97,7 +103,7 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
     X.pad_ = 0;
     // baby-step start tables: A[l] = s^(C*l), B[w] = s^(32*C*w)
     u64 *tb = tabs + (size_t)t * TABS;
-    const u64 u = mpow(s, (u64)BSGS_C, M);
+    const u64 u = mpow(s, (u64)gm.c, M);
     u64 a = M.one;
     for (int l = 0; l < 32; ++l) { tb[l] = a; a = mmul(a, u, p, M.q); }
     const u64 v = a;                                      // u^32
@@ -112,10 +118,11 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
 }
 
 // Kernel 2: one warp per prime; lanes walk the sequences.
-__global__ void __launch_bounds__(SETUP_TPB) k_setup_k(const JobDev *__restrict__ job, PrimeHdr *__restrict__ hdr,
+__global__ void __launch_bounds__(SETUP_TPB, 6) k_setup_k(const JobDev *__restrict__ job, PrimeHdr *__restrict__ hdr,
                                                        const PrimeAux *__restrict__ aux, u32 count,
                                                        u64 *__restrict__ tabs, u64 *__restrict__ tgt,
-                                                       unsigned char *__restrict__ meta, u64 *__restrict__ stats)
+                                                       unsigned char *__restrict__ meta, u64 *__restrict__ stats,
+                                                       SetupGeom gm)
 {
     const u32 lane = threadIdx.x & 31;
     const u32 w = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5;
@@ -186,9 +193,9 @@ __global__ void __launch_bounds__(SETUP_TPB) k_setup_k(const JobDev *__restrict_
         }
         return;
     }
-    // giant-phase split: G chunks of Lc giant steps per target, numk*G <= BSGS_TPB
-    const u32 Mg = (H.e == 2) ? job->M2 : job->M1;
-    u32 G = BSGS_TPB / nk;
+    // giant-phase split: G chunks of Lc giant steps per target, numk*G <= tpb
+    const u32 Mg = (H.e == 2) ? gm.m2 : gm.m1;
+    u32 G = gm.tpb / nk;
     if (G < 1) G = 1;
     if (G > Mg) G = Mg;
     const u32 Lc = (Mg + G - 1) / G;
@@ -222,15 +229,20 @@ __global__ void __launch_bounds__(SETUP_TPB) k_setup_k(const JobDev *__restrict_
 }
 
 cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 count, PrimeHdr *hdr, void *aux, u64 *tabs,
-                         u64 *tgt, unsigned char *meta, u64 *stats, cudaStream_t st)
+                         u64 *tgt, unsigned char *meta, u64 *stats, int geom, u32 L, cudaStream_t st)
 {
     if (count == 0) return cudaSuccess;
-    k_setup_prime<<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, tabs);
+    const BsgsGeom &g = BSGS_GEOMS[geom];
+    SetupGeom gm;
+    gm.q = g.q; gm.c = g.c; gm.tpb = g.tpb;
+    gm.m1 = (u32)(((u64)L + g.q - 1) / g.q);
+    gm.m2 = (u32)(((u64)L + 2ull * g.q - 1) / (2ull * g.q));
+    k_setup_prime<<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, tabs, gm);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const u32 wpb = SETUP_TPB / 32;
     k_setup_k<<<(count + wpb - 1) / wpb, SETUP_TPB, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, tgt, meta,
-                                                            stats);
+                                                            stats, gm);
     return cudaGetLastError();
 }
 

@@ -88,3 +88,43 @@ def test_long_n_range_many_giant_chunks(sieve, oracle, rs, seed, kcount, base):
     Bases 3 and 7 take the general baby step (b^e added or multiplied)."""
     job = W.small_job(seed, kcount=kcount, base=base, nmin=1_000_000, nmax=4_999_999, keep=0.05, kmax=1 << 28)
     _check_job(sieve, oracle, job, 3_000_000, 3_004_000, rs)
+
+
+@pytest.mark.parametrize("q", [1024, 2048, 4096, 8192, 16384])
+def test_every_baby_step_geometry(sieve, oracle, rs, q):
+    """Each BSGS geometry (Q baby steps, its table and block size) against the
+    brute-force oracle: dense factors at small p (small orders, table rebuilds)
+    and 100 sequences over a long n-range (many giant chunks per target)."""
+    sieve.set_baby_steps(q)
+    try:
+        job = W.small_job(41, kcount=24, base=2, nmin=1000, nmax=30000, keep=0.4, kmax=1 << 24)
+        _check_job(sieve, oracle, job, 3, 100_000, rs)
+        assert sieve.baby_steps() == (q, False)
+        job = W.small_job(42, kcount=100, base=2, nmin=1_000_000, nmax=2_999_999, keep=0.05, kmax=1 << 28)
+        _check_job(sieve, oracle, job, 3_000_000, 3_002_000, rs)
+    finally:
+        sieve.set_baby_steps(0)
+
+
+def test_tuner_runs_candidates_and_matches_fixed_q(sieve, rs):
+    """Automatic Q: the first chunks run the candidate geometries in turn and the
+    tuner settles on one; the eliminated terms equal a run with Q fixed."""
+    job = W.small_job(43, kcount=8, base=2, nmin=100000, nmax=299999, keep=0.06, kmax=1 << 20, signs=-1)
+    p0, p1 = 10 ** 12, 10 ** 12 + 60_000_000          # about 2.2e6 primes, 17 chunks
+    sieve.set_baby_steps(0)
+    sieve.load(W.seqs_of(job))
+    assert sieve.baby_steps()[1]                     # tuning at the start
+    cnt_auto = sieve.run(p0, p1)
+    q_auto, tuning = sieve.baby_steps()
+    assert not tuning and q_auto in rs.BABY_STEPS
+    fa, bma = sieve.factors(), sieve.bitmap()
+    sieve.set_baby_steps(16384)
+    try:
+        sieve.load(W.seqs_of(job))
+        cnt_fixed = sieve.run(p0, p1)
+        ff, bmf = sieve.factors(), sieve.bitmap()
+    finally:
+        sieve.set_baby_steps(0)
+    assert cnt_auto["primes"] == cnt_fixed["primes"]
+    assert set(zip(fa["seq"].tolist(), fa["n"].tolist())) == set(zip(ff["seq"].tolist(), ff["n"].tolist()))
+    assert np.array_equal(bma, bmf)
