@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--baby-steps", type=int, default=0, help="fix Q baby steps per prime (0: the per-job tuner)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     return ap.parse_args()
 
@@ -187,6 +188,7 @@ def main():
     sv = rs.Sieve(local)
     sv.set_stream(stream.cuda_stream)
     peak = sv.mulmod_peak()
+    sv.set_baby_steps(args.baby_steps)
     sv.load(seqs)
     width = 1 << args.width
     # disjoint windows per rank: rank r takes windows r, r+world, ...
@@ -197,6 +199,7 @@ def main():
     for i in range(args.warmup):
         sv.run(*windows[i])
     sv.factors()
+    baby_q, tuning = sv.baby_steps()                  # the per-job tuner settles during the warm-up
     torch.cuda.synchronize()
     barrier()
 
@@ -273,6 +276,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "p_window_log2": args.width, "seed": args.seed,
+                       "baby_steps": baby_q, "baby_steps_tuned": not tuning,
                        "l2": "flushed between steps (256 MiB write outside the step events)",
                        "parallelism": "p-range windows per rank" if world > 1 else "1 GPU"},
             "e2e": e2e,

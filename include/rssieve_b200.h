@@ -149,7 +149,9 @@ int rs_device_count(void);
  * are built (cl_sieve.cpp:893-938).  In automatic mode a model of the per-prime
  * cost keeps the candidates within 2x of its best, the first full chunks of
  * the job run with each in turn (their results count, as every Q is exact),
- * and the fastest measured one is kept.  Takes effect at once. */
+ * and the fastest measured one is kept; later jobs of the same shape (base,
+ * sequence count, n-range length) on the context reuse it.  Takes effect at
+ * once. */
 int rs_set_baby_steps(rs_ctx *ctx, uint32_t q);
 /* The Q in use; *tuning (may be NULL) is 1 while candidates are being timed. */
 int rs_get_baby_steps(rs_ctx *ctx, uint32_t *q, int *tuning);

@@ -58,6 +58,7 @@ struct rs_ctx {
     double tune_ms[NGEOM];
     u64 tune_primes[NGEOM];
     std::vector<int> chunk_geom;
+    std::vector<std::pair<u64, int>> tuned;   // job shape (base, kcount, L) -> tuned geometry
     // timing of the last rs_run_range
     std::vector<cudaEvent_t> ev;
     double last_bsgs_ms = 0, last_total_ms = 0;
@@ -206,6 +207,12 @@ static double geom_model_cost(int g, u32 kcount, u32 L)
     return 1.15 * q + 1.2 * giant;
 }
 
+// Jobs of one shape share a tuned geometry (a reloaded or resumed job skips tuning).
+static u64 job_shape(const rs_ctx *c)
+{
+    return ((u64)c->h_job.base << 40) ^ ((u64)c->h_job.kcount << 32) ^ (u64)c->h_job.L;
+}
+
 // Starts the per-job tuner: the candidates are the geometries whose model cost
 // is within 2x of the model's best; the first chunks cycle through them.
 static void tune_start(rs_ctx *c)
@@ -228,6 +235,8 @@ static void tune_start(rs_ctx *c)
         if (geom_model_cost(g, c->h_job.kcount, c->h_job.L) <= 2.0 * best) c->tune_cand[c->tune_ncand++] = g;
     c->geom = gb;
     c->tuning = (c->tune_ncand > 1);
+    for (const auto &t : c->tuned)
+        if (t.first == job_shape(c)) { c->geom = t.second; c->tuning = false; }
 }
 
 // Records one chunk's BSGS time; ends tuning once every candidate has timed at
@@ -246,6 +255,7 @@ static void tune_record(rs_ctx *c, int g, u32 primes, float ms)
         if (v < best) { best = v; c->geom = gi; }
     }
     c->tuning = false;
+    c->tuned.emplace_back(job_shape(c), c->geom);
 }
 
 extern "C" int rs_set_baby_steps(rs_ctx *c, uint32_t q)
