@@ -175,6 +175,38 @@ int rs_primes_generate(rs_ctx *ctx, uint64_t p0, uint64_t p1, uint64_t *dst, siz
 int rs_last_timing(rs_ctx *ctx, double *bsgs_ms, double *total_kernel_ms, uint32_t *bsgs_launches,
                    uint32_t *kernel_launches);
 
+/* ---------------- batches: many jobs on one device ----------------
+ * The reference sieves one job per process (cl_sieve.cpp:975-1451).  A batch
+ * holds many independent jobs -- own sequences, n-range, bitmap and p-range
+ * each -- and advances all of them in rounds of device-resident work: every
+ * unfinished job sieves its next window (about 39 000 primes) per round, the
+ * BSGS work of all jobs that share a geometry runs in one persistent launch,
+ * and the host waits once per round.  After the first round a round is
+ * replayed from a captured CUDA graph.  Each job's eliminated terms equal what
+ * rs_run_range gives for the same job and p-range. */
+typedef struct rs_batch rs_batch;
+int rs_batch_create(int device, rs_batch **out);
+void rs_batch_destroy(rs_batch *b);
+/* A caller stream (cudaStream_t as void*, not the legacy NULL stream); only
+ * before the first rs_batch_run. */
+int rs_batch_set_stream(rs_batch *b, void *stream);
+/* Adds a job with its p-range [p0, p1) (3 <= p0 < p1); q fixes its baby-step
+ * count (as rs_set_baby_steps) or 0 takes the cost model's choice.  The job's
+ * bitmap is copied.  *job (may be NULL) receives its index.  Only before the
+ * first rs_batch_run. */
+int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t p1, uint32_t q, uint32_t *job);
+/* Runs up to max_rounds rounds (0: until every job is done); *done = 1 once
+ * every job's p-range is finished. */
+int rs_batch_run(rs_batch *b, uint32_t max_rounds, int *done);
+/* Per job, as rs_factors_fetch / rs_bitmap_download. */
+int rs_batch_factors_fetch(rs_batch *b, uint32_t job, rs_factor *buf, size_t cap, size_t *n);
+int rs_batch_bitmap_download(rs_batch *b, uint32_t job, uint32_t *dst, size_t words);
+/* A job's baby-step count, primes tested so far and whether its range is done
+ * (each pointer may be NULL). */
+int rs_batch_job_info(rs_batch *b, uint32_t job, uint32_t *q, uint64_t *primes, int *done);
+/* Counters summed over the batch's jobs. */
+int rs_batch_counters(rs_batch *b, rs_counters *out);
+
 /* Throughput of independent 64-bit Montgomery products (the kernels' mmul)
  * on this device, in 10^9 products/s: the roofline denominator of the
  * integer-multiply-bound BSGS kernel. */

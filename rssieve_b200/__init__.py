@@ -52,6 +52,8 @@ EXPORTS = (
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
     "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_primes_generate_noalloc",
     "rs_set_baby_steps", "rs_get_baby_steps",
+    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_run",
+    "rs_batch_factors_fetch", "rs_batch_bitmap_download", "rs_batch_job_info", "rs_batch_counters",
 )
 BABY_STEPS = (1024, 2048, 4096, 8192, 16384)   # accepted by rs_set_baby_steps (0: automatic)
 NOALLOC_MAX_WIDTH = 1 << 22     # RS_NOALLOC_MAX_WIDTH
@@ -103,6 +105,15 @@ def lib():
         "rs_mulmod_peak": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "rs_primes_generate_noalloc": (C.c_int, [u64, u64, vp, u32, vp, vp]),
         "rs_set_baby_steps": (C.c_int, [vp, u32]),
+        "rs_batch_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+        "rs_batch_destroy": (None, [vp]),
+        "rs_batch_set_stream": (C.c_int, [vp, vp]),
+        "rs_batch_add": (C.c_int, [vp, PS, u64, u64, u32, C.POINTER(u32)]),
+        "rs_batch_run": (C.c_int, [vp, u32, C.POINTER(C.c_int)]),
+        "rs_batch_factors_fetch": (C.c_int, [vp, u32, vp, sz, C.POINTER(sz)]),
+        "rs_batch_bitmap_download": (C.c_int, [vp, u32, vp, sz]),
+        "rs_batch_job_info": (C.c_int, [vp, u32, C.POINTER(u32), C.POINTER(u64), C.POINTER(C.c_int)]),
+        "rs_batch_counters": (C.c_int, [vp, C.POINTER(_Counters)]),
         "rs_get_baby_steps": (C.c_int, [vp, C.POINTER(u32), C.POINTER(C.c_int)]),
     }
     for name, (res, args) in sig.items():
@@ -338,6 +349,67 @@ class Sieve:
         bl, kl = C.c_uint32(0), C.c_uint32(0)
         _check(lib().rs_last_timing(self._c, C.byref(b), C.byref(t), C.byref(bl), C.byref(kl)), "rs_last_timing")
         return {"bsgs_ms_avg": b.value, "total_ms": t.value, "bsgs_launches": bl.value, "kernel_launches": kl.value}
+
+
+class Batch:
+    """Many independent jobs sieved together on one device (rs_batch_*)."""
+
+    def __init__(self, device=0):
+        L = lib()
+        self._b = C.c_void_p()
+        _check(L.rs_batch_create(device, C.byref(self._b)), "rs_batch_create")
+        self._seqs = []
+
+    def close(self):
+        if getattr(self, "_b", None) and self._b.value:
+            lib().rs_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, seqs, p0, p1, q=0):
+        """Add a job over [p0, p1); returns its index."""
+        j = C.c_uint32(0)
+        _check(lib().rs_batch_add(self._b, seqs._p, p0, p1, q, C.byref(j)), "rs_batch_add")
+        self._seqs.append(seqs)
+        return j.value
+
+    def run(self, max_rounds=0):
+        """Run up to max_rounds rounds (0: to completion); True once every job is done."""
+        d = C.c_int(0)
+        _check(lib().rs_batch_run(self._b, max_rounds, C.byref(d)), "rs_batch_run")
+        return bool(d.value)
+
+    def factors(self, job):
+        L = lib()
+        n = C.c_size_t(0)
+        rc = L.rs_batch_factors_fetch(self._b, job, None, 0, C.byref(n))
+        if rc not in (RS_OK, RS_EARG):
+            _check(rc, "rs_batch_factors_fetch")
+        out = np.zeros(max(n.value, 1), dtype=FACTOR_DT)
+        _check(L.rs_batch_factors_fetch(self._b, job, out.ctypes.data, len(out), C.byref(n)), "rs_batch_factors_fetch")
+        return out[: n.value].copy()
+
+    def bitmap(self, job):
+        s = self._seqs[job]
+        out = np.zeros(s.kcount * s.words_per_seq, dtype=np.uint32)
+        _check(lib().rs_batch_bitmap_download(self._b, job, out.ctypes.data, len(out)), "rs_batch_bitmap_download")
+        return out.reshape(s.kcount, s.words_per_seq)
+
+    def job_info(self, job):
+        """(baby steps Q, primes tested, done)."""
+        q, n, d = C.c_uint32(0), C.c_uint64(0), C.c_int(0)
+        _check(lib().rs_batch_job_info(self._b, job, C.byref(q), C.byref(n), C.byref(d)), "rs_batch_job_info")
+        return q.value, n.value, bool(d.value)
+
+    def counters(self):
+        d = _Counters()
+        _check(lib().rs_batch_counters(self._b, C.byref(d)), "rs_batch_counters")
+        return {f: int(getattr(d, f)) for f in COUNTER_FIELDS}
 
 
 def term_set(factors):

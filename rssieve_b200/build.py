@@ -22,7 +22,7 @@ LIB = os.path.join(LIBDIR, "librssieve_b200.so")
 CLI = os.path.join(LIBDIR, "rssieve")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["sieve.cu", "setup.cu", "bsgs.cu", "peak.cu", "engine.cu", "noalloc.cu"]
+CU_SOURCES = ["sieve.cu", "setup.cu", "bsgs.cu", "peak.cu", "engine.cu", "noalloc.cu", "batch.cu"]
 CPP_SOURCES = ["host.cpp"]
 HEADERS = ["mont.cuh", "rs_internal.h", "rs_host.h"]
 

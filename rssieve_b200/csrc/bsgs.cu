@@ -372,14 +372,37 @@ __device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
     }
 }
 
+// Work item i of a batch launch: the group's ranges hold prefix[k+1]-prefix[k]
+// primes each, in record slots range*rcap + (0, 1, ...).
+__device__ __forceinline__ u32 batch_slot(u32 i, const u32 *granges, u32 nr, const u32 *prefix, u32 rcap)
+{
+    u32 lo = 0, hi = nr;                 // last k with prefix[k] <= i
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (prefix[mid] <= i) lo = mid; else hi = mid;
+    }
+    return granges[lo] * rcap + (i - prefix[lo]);
+}
+
 // MODE: 1 = every prime below 2^63 (Shoup giant steps), 0 = every prime at or
 // above 2^63 (Montgomery giant steps).  1024 / TPB CTAs share an SM, so the
-// bound keeps each thread at 64 registers.
-template <int TPB, int C, int NB, int MODE>
+// bound keeps each thread at 64 registers.  BATCH: the primes of several
+// ranges (jobs) in one launch -- work item i maps to a record slot through the
+// group's prefix sums, and each prime's job arguments come from job_args.
+template <int TPB, int C, int NB, int MODE, bool BATCH>
 __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const PrimeHdr *__restrict__ hdr,
                                                  const u64 *__restrict__ tabs, const u64 *__restrict__ tgt,
-                                                 const unsigned char *__restrict__ meta, u32 count, u32 *work_ctr)
+                                                 const unsigned char *__restrict__ meta, u32 count, u32 *work_ctr,
+                                                 const BsgsArgs *__restrict__ job_args,
+                                                 const u32 *__restrict__ granges, u32 nr,
+                                                 const u32 *__restrict__ prefix, u32 rcap)
 {
+    constexpr u32 NONE = 0xFFFFFFFFu;
+    if (BATCH) count = prefix[nr];
+    auto slot_of = [&](u32 i) -> u32 {
+        if (i >= count) return NONE;
+        return BATCH ? batch_slot(i, granges, nr, prefix, rcap) : i;
+    };
     constexpr u32 Q = TPB * C;
     static_assert(Q <= 65536, "baby indices are stored in 16 bits");
     constexpr int IB = 8;                                         // values inserted per batch
@@ -409,16 +432,16 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         s_cands = 0;
         s_dups = 0;
         s_facs = 0;
-        const u32 i0 = atomicAdd(work_ctr, 1u);
+        const u32 i0 = slot_of(atomicAdd(work_ctr, 1u));
         s_idx[0] = i0;
-        if (i0 < count) fetch(0, i0);
+        if (i0 != NONE) fetch(0, i0);
     }
     __syncthreads();
 
     for (u32 it = 0;; ++it) {
         const u32 buf = it & 1;
         const u32 idx = s_idx[buf];
-        if (idx >= count) break;
+        if (idx == NONE) break;
         // this prime's record was fetched one prime ago; the wait is bounded
         {
             u32 n = 0;
@@ -438,14 +461,15 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             s_nsol = 0;
             s_spill = 0;
             s_ctx.p = p; s_ctx.q = q; s_ctx.s = s; s_ctx.smul = smul; s_ctx.e = e;
-            nxt = atomicAdd(work_ctr, 1u);
+            if (BATCH) s_args = job_args[R.hdr.job];
+            nxt = slot_of(atomicAdd(work_ctr, 1u));
         }
         if (live) clear_table(T, NB);
         __syncthreads();
         if (s_abort) break;
         if (tid == 0) {
             s_idx[buf ^ 1] = nxt;
-            if (nxt < count) {                                    // rec[buf^1] was last read before the previous barrier
+            if (nxt != NONE) {                                    // rec[buf^1] was last read before the previous barrier
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 fetch(buf ^ 1, nxt);
             }
@@ -494,7 +518,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         }
         __syncthreads();
         const u32 order = s_order;
-        const u32 Mg = (e == 2) ? a.M2 : a.M1;
+        const u32 Mg = (e == 2) ? s_args.M2 : s_args.M1;
         if (live) {
             if (order < Q) rebuild_table<TPB, C, NB>(order);
             else if (tid == 0 && s_spill) atomicOr(a.err, ERR_HASH_OVERFLOW);
@@ -567,12 +591,14 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
     }
 }
 
-template <int G, int MODE>
+template <int G, int MODE, bool BATCH = false>
 static cudaError_t launch_geom(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
-                              const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st)
+                              const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st,
+                              const BsgsArgs *job_args = nullptr, const u32 *granges = nullptr, u32 nr = 0,
+                              const u32 *prefix = nullptr, u32 rcap = 0)
 {
     constexpr BsgsGeom g = BSGS_GEOMS[G];
-    auto kern = k_bsgs<g.tpb, g.c, g.nb, MODE>;
+    auto kern = k_bsgs<g.tpb, g.c, g.nb, MODE, BATCH>;
     const size_t smem = Smem<g.tpb, g.nb>::bytes();
     static thread_local int per_sm[32] = {0};            // resident CTAs per SM, per device
     int dev = 0;
@@ -584,8 +610,8 @@ static cudaError_t launch_geom(const BsgsArgs &a, const PrimeHdr *hdr, const u64
         if (occ < 1) return cudaErrorInvalidConfiguration;
     }
     const u64 want = (u64)sms * (u64)occ;
-    const unsigned grid = (unsigned)((want < count) ? want : count);
-    kern<<<grid, g.tpb, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr);
+    const unsigned grid = (unsigned)((BATCH || want < count) ? want : count);
+    kern<<<grid, g.tpb, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr, job_args, granges, nr, prefix, rcap);
     return cudaGetLastError();
 }
 
@@ -593,7 +619,10 @@ template <int G, int MODE>
 static cudaError_t set_smem()
 {
     constexpr BsgsGeom g = BSGS_GEOMS[G];
-    return cudaFuncSetAttribute(k_bsgs<g.tpb, g.c, g.nb, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_bsgs<g.tpb, g.c, g.nb, MODE, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Smem<g.tpb, g.nb>::bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_bsgs<g.tpb, g.c, g.nb, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)Smem<g.tpb, g.nb>::bytes());
 }
 
@@ -644,6 +673,44 @@ cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs,
     default: return cudaErrorInvalidValue;
     }
 #undef RS_BSGS_CASE
+}
+
+// prefix[0] = 0, prefix[k+1] = prefix[k] + primes of the group's k-th range (one thread)
+__global__ void k_batch_prefix(const u32 *granges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix)
+{
+    u32 acc = 0;
+    prefix[0] = 0;
+    for (u32 k = 0; k < nr; ++k) {
+        acc += min(ctrs[granges[k] * BR_CTRS + 1], rcap);
+        prefix[k + 1] = acc;
+    }
+}
+
+cudaError_t launch_batch_prefix(const u32 *group_ranges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix, cudaStream_t st)
+{
+    k_batch_prefix<<<1, 1, 0, st>>>(group_ranges, nr, ctrs, rcap, prefix);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
+                              const u64 *tgt, const unsigned char *meta, const u32 *group_ranges, u32 nr,
+                              const u32 *prefix, u32 rcap, u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st)
+{
+#define RS_BSGS_BCASE(G)                                                                                         \
+    case G:                                                                                                      \
+        return shoup ? launch_geom<G, 1, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, group_ranges, \
+                                               nr, prefix, rcap)                                                 \
+                     : launch_geom<G, 0, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, group_ranges, \
+                                               nr, prefix, rcap);
+    switch (geom) {
+        RS_BSGS_BCASE(0)
+        RS_BSGS_BCASE(1)
+        RS_BSGS_BCASE(2)
+        RS_BSGS_BCASE(3)
+        RS_BSGS_BCASE(4)
+    default: return cudaErrorInvalidValue;
+    }
+#undef RS_BSGS_BCASE
 }
 
 }  // namespace rs

@@ -83,7 +83,7 @@ static void free_job(rs_ctx *c)
     c->job_loaded = false;
 }
 
-static std::vector<u32> small_primes()
+std::vector<u32> rs_small_primes()
 {
     std::vector<u32> v;
     std::vector<char> comp(65536, 0);
@@ -148,7 +148,7 @@ extern "C" int rs_ctx_create(int device, rs_ctx **out)
     c->sms = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) return fail(RS_ECUDA);
     c->stream = c->own;
-    std::vector<u32> sp = small_primes();
+    std::vector<u32> sp = rs_small_primes();
     c->nsp = (u32)sp.size();
     c->cand_cap = 1u << 24;
     c->prime_cap = 1u << 24;
@@ -193,18 +193,6 @@ static void odd_split(u64 x, u64 &odd, u32 &v2)
     v2 = 0;
     while (!(x & 1)) { x >>= 1; ++v2; }
     odd = x;
-}
-
-// Model cost of one prime for a geometry, in baby-step units: Q baby steps plus
-// the giant steps of the targets that survive the prefilter (about 0.6 of the
-// sequences; half the primes use the parity split, which halves their range),
-// a giant step costing about 1.2 baby steps, and the per-prime fixed work
-// (table clear, barriers) of about 0.15 Q.
-static double geom_model_cost(int g, u32 kcount, u32 L)
-{
-    const double q = BSGS_GEOMS[g].q;
-    const double giant = 0.6 * kcount * 0.75 * std::ceil((double)L / q);
-    return 1.15 * q + 1.2 * giant;
 }
 
 // Jobs of one shape share a tuned geometry (a reloaded or resumed job skips tuning).
@@ -278,6 +266,27 @@ extern "C" int rs_get_baby_steps(rs_ctx *c, uint32_t *q, int *tuning)
     return RS_OK;
 }
 
+// Device record of a job: sequences, n-range, odd parts and Barrett
+// reciprocals of every k and of the base (bitmap pointer left null).
+void jobdev_from_seqs(const rs_seqs *s, JobDev *out)
+{
+    memset(out, 0, sizeof *out);
+    out->base = s->base;
+    out->kcount = s->kcount;
+    out->nmin = s->nmin;
+    out->nmax = s->nmax;
+    out->L = s->nmax - s->nmin + 1;
+    out->words = (u32)s->words_per_seq;
+    for (u32 i = 0; i < s->kcount; ++i) {
+        out->k[i] = s->k[i];
+        out->c[i] = s->c[i];
+        odd_split(s->k[i], out->kodd[i], out->kv2[i]);
+        out->krd[i] = ~0ull / out->kodd[i];
+    }
+    odd_split(s->base, out->bodd, out->bv2);
+    out->brd = ~0ull / out->bodd;
+}
+
 extern "C" int rs_job_load(rs_ctx *c, const rs_seqs *s)
 {
     if (!c || !s) return RS_EARG;
@@ -286,21 +295,7 @@ extern "C" int rs_job_load(rs_ctx *c, const rs_seqs *s)
     CU(cudaSetDevice(c->device));
     free_job(c);
     JobDev J;
-    memset(&J, 0, sizeof J);
-    J.base = s->base;
-    J.kcount = s->kcount;
-    J.nmin = s->nmin;
-    J.nmax = s->nmax;
-    J.L = s->nmax - s->nmin + 1;
-    J.words = (u32)s->words_per_seq;
-    for (u32 i = 0; i < s->kcount; ++i) {
-        J.k[i] = s->k[i];
-        J.c[i] = s->c[i];
-        odd_split(s->k[i], J.kodd[i], J.kv2[i]);
-        J.krd[i] = ~0ull / J.kodd[i];
-    }
-    odd_split(s->base, J.bodd, J.bv2);
-    J.brd = ~0ull / J.bodd;
+    jobdev_from_seqs(s, &J);
     c->bitmap_words = (size_t)s->kcount * s->words_per_seq;
     uint64_t cand = rs_seqs_count(s);
     c->factor_cap = (u32)std::min<uint64_t>(cand + 1, 0xFFFFFFF0ull);

@@ -7,6 +7,7 @@
 // power tables, BSGS targets) that the BSGS kernel consumes.
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace rs {
@@ -36,6 +37,25 @@ constexpr BsgsGeom BSGS_GEOMS[NGEOM] = {
 constexpr int geom_index(u32 q)
 {
     return q == 16384 ? 0 : q == 8192 ? 1 : q == 4096 ? 2 : q == 2048 ? 3 : q == 1024 ? 4 : -1;
+}
+
+// Model cost of one prime for a geometry, in baby-step units: Q baby steps plus
+// the giant steps of the targets that survive the prefilter (about 0.6 of the
+// sequences; half the primes use the parity split, which halves their range),
+// a giant step costing about 1.2 baby steps, and the per-prime fixed work
+// (table clear, barriers) of about 0.15 Q.
+inline double geom_model_cost(int g, u32 kcount, u32 L)
+{
+    const double q = BSGS_GEOMS[g].q;
+    const double m = ((double)L + q - 1) / q;
+    return 1.15 * q + 1.2 * 0.6 * kcount * 0.75 * (double)(u64)m;
+}
+inline int geom_model_best(u32 kcount, u32 L)
+{
+    int best = 0;
+    for (int g = 1; g < NGEOM; ++g)
+        if (geom_model_cost(g, kcount, L) < geom_model_cost(best, kcount, L)) best = g;
+    return best;
 }
 constexpr int BSGS_MAXPROBE = 64;
 constexpr int BSGS_SPEC_PROBE = 64;         // bucket walk bound while ord(s) is still unknown
@@ -95,7 +115,7 @@ struct PrimeHdr {        // 80 bytes (a 16-byte multiple: copied by TMA bulk cop
     u32 e;               // 1 or 2
     u32 G, Lc;           // giant phase: G chunks of Lc giant steps
     u32 smul;            // b^e as an integer when the baby step uses additions, else 0
-    u32 pad_;
+    u32 job;             // job index within a batch (0 for a single job)
     u64 Sh;              // Montgomery S^(Lc/2): start of a thread's second giant chain
     u64 Sw;              // floor(Sp*2^64/p), Sp = s^Q mod p (plain), for Shoup giant steps; 0 when p >= 2^63
 };
@@ -118,6 +138,23 @@ struct BsgsArgs {
     u32 *err;
 };
 
+// ---- batches: many jobs, each with one or more p-ranges, advanced in rounds ----
+// A range's window of one round, written on the device by k_batch_windows.
+struct BatchWin {
+    u64 lo, hi;          // this round's [lo, hi) (lo == hi: the range is done)
+    u64 base_odd, nodd;  // odd values base_odd + 2i, i < nodd, covering [lo, hi)
+};
+struct BatchRange {      // device state of one range
+    u64 p_cur, p_end;    // next window start, end of the range
+    u32 job, pad_;
+};
+// per-range counters of a round: [0] sieve survivors, [1] primes, [2] pad, [3] pad
+constexpr int BR_CTRS = 4;
+// per-job BSGS geometry as the set-up kernels need it
+struct JobGeom {
+    u32 q, c, tpb, m1, m2, pad_;
+};
+
 // launch wrappers (sieve.cu, setup.cu, bsgs.cu)
 cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp, u64 *cands, u32 cand_cap,
                          u32 *ctrs, u32 *err, cudaStream_t st);
@@ -134,4 +171,25 @@ size_t bsgs_smem_bytes(int geom);
 cudaError_t bsgs_prepare();   // per device, before the first launch
 cudaError_t launch_mulmod_peak(u64 *out, int blocks, int iters, cudaStream_t st);
 
+// batch rounds (sieve.cu, setup.cu, bsgs.cu)
+cudaError_t launch_batch_windows(BatchRange *ranges, BatchWin *wins, u32 nranges, u32 rcap, u32 *ctrs, cudaStream_t st);
+cudaError_t launch_sieve_batch(const BatchWin *wins, u32 nranges, u32 max_blocks, const u32 *sp, u32 nsp, u64 *cands,
+                               u32 ccap, u32 *ctrs, u32 *err, cudaStream_t st);
+cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges, u32 *err,
+                            int sms, cudaStream_t st);
+cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
+                               u32 rcap, const u32 *ctrs, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs, u64 *tgt,
+                               unsigned char *meta, u64 *stats, cudaStream_t st);
+// one BSGS launch over the ranges of one (geometry, mode) group: group_ranges
+// lists them, prefix (nr+1 entries) is filled by launch_batch_prefix
+cudaError_t launch_batch_prefix(const u32 *group_ranges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix, cudaStream_t st);
+cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
+                              const u64 *tgt, const unsigned char *meta, const u32 *group_ranges, u32 nr,
+                              const u32 *prefix, u32 rcap, u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st);
+
 }  // namespace rs
+
+// host helpers shared by engine.cu and batch.cu
+struct rs_seqs;
+std::vector<rs::u32> rs_small_primes();                       // odd primes below 2^16, ascending
+void jobdev_from_seqs(const rs_seqs *s, rs::JobDev *out);    // JobDev of a job (bitmap pointer null)

@@ -62,21 +62,37 @@ struct PrimeAux {        // kernel 1 -> kernel 2 scalars
     u32 pad_;
 };
 
-// The BSGS geometry of a launch: Q = tpb * c baby steps, and the giant steps
-// per target that Q implies.
-struct SetupGeom {
-    u32 q, c, tpb, m1, m2;
-};
-
-__global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ job, const u64 *__restrict__ primes,
+// Kernel 1.  Single job: primes[first, first+count) into records [0, count)
+// with the launch's geometry gm.  Batch (BATCH): blockIdx.y is the range; its
+// job, geometry, prime count and record slots come from the batch tables.
+template <bool BATCH>
+__global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ jobs, const u64 *__restrict__ primes,
                                                      u32 first, u32 count, PrimeHdr *__restrict__ hdr,
-                                                     PrimeAux *__restrict__ aux, u64 *__restrict__ tabs, SetupGeom gm)
+                                                     PrimeAux *__restrict__ aux, u64 *__restrict__ tabs, JobGeom gm,
+                                                     const JobGeom *__restrict__ geoms,
+                                                     const BatchRange *__restrict__ ranges,
+                                                     const u32 *__restrict__ ctrs, u32 rcap)
 {
+    const JobDev *job = jobs;
+    u32 jb = 0;
+    if (BATCH) {
+        const u32 r = blockIdx.y;
+        jb = ranges[r].job;
+        job = jobs + jb;
+        gm = geoms[jb];
+        count = min(ctrs[r * BR_CTRS + 1], rcap);
+        const size_t off = (size_t)r * rcap;
+        primes += off;
+        hdr += off;
+        aux += off;
+        tabs += off * TABS;
+        first = 0;
+    }
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
     const u64 p = primes[first + t];
     PrimeHdr H;
-    H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.pad_ = 0;
+    H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.job = jb;
     H.Sh = 0; H.Sw = 0;
     const Mont M = mont_init(p);
     const u32 b = job->base;
@@ -117,13 +133,30 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
     aux[t] = X;
 }
 
-// Kernel 2: one warp per prime; lanes walk the sequences.
-__global__ void __launch_bounds__(SETUP_TPB, 6) k_setup_k(const JobDev *__restrict__ job, PrimeHdr *__restrict__ hdr,
+// Kernel 2: one warp per prime; lanes walk the sequences.  BATCH as kernel 1.
+template <bool BATCH>
+__global__ void __launch_bounds__(SETUP_TPB, 6) k_setup_k(const JobDev *__restrict__ jobs, PrimeHdr *__restrict__ hdr,
                                                        const PrimeAux *__restrict__ aux, u32 count,
                                                        u64 *__restrict__ tabs, u64 *__restrict__ tgt,
                                                        unsigned char *__restrict__ meta, u64 *__restrict__ stats,
-                                                       SetupGeom gm)
+                                                       JobGeom gm, const JobGeom *__restrict__ geoms,
+                                                       const BatchRange *__restrict__ ranges,
+                                                       const u32 *__restrict__ ctrs, u32 rcap)
 {
+    const JobDev *job = jobs;
+    if (BATCH) {
+        const u32 r = blockIdx.y;
+        const u32 jb = ranges[r].job;
+        job = jobs + jb;
+        gm = geoms[jb];
+        count = min(ctrs[r * BR_CTRS + 1], rcap);
+        const size_t off = (size_t)r * rcap;
+        hdr += off;
+        aux += off;
+        tabs += off * TABS;
+        tgt += off * KSTRIDE;
+        meta += off * KSTRIDE;
+    }
     const u32 lane = threadIdx.x & 31;
     const u32 w = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5;
     if (w >= count) return;
@@ -233,16 +266,32 @@ cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 co
 {
     if (count == 0) return cudaSuccess;
     const BsgsGeom &g = BSGS_GEOMS[geom];
-    SetupGeom gm;
-    gm.q = g.q; gm.c = g.c; gm.tpb = g.tpb;
+    JobGeom gm;
+    gm.q = g.q; gm.c = g.c; gm.tpb = g.tpb; gm.pad_ = 0;
     gm.m1 = (u32)(((u64)L + g.q - 1) / g.q);
     gm.m2 = (u32)(((u64)L + 2ull * g.q - 1) / (2ull * g.q));
-    k_setup_prime<<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, tabs, gm);
+    k_setup_prime<false><<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, tabs, gm,
+                                                              nullptr, nullptr, nullptr, 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const u32 wpb = SETUP_TPB / 32;
-    k_setup_k<<<(count + wpb - 1) / wpb, SETUP_TPB, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, tgt, meta,
-                                                            stats, gm);
+    k_setup_k<false><<<(count + wpb - 1) / wpb, SETUP_TPB, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, tgt,
+                                                                   meta, stats, gm, nullptr, nullptr, nullptr, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
+                               u32 rcap, const u32 *ctrs, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs, u64 *tgt,
+                               unsigned char *meta, u64 *stats, cudaStream_t st)
+{
+    JobGeom gm{};
+    k_setup_prime<true><<<dim3((rcap + 255) / 256, nranges), 256, 0, st>>>(jobs, primes, 0, 0, hdr, (PrimeAux *)aux,
+                                                                           tabs, gm, geoms, ranges, ctrs, rcap);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const u32 wpb = SETUP_TPB / 32;
+    k_setup_k<true><<<dim3((rcap + wpb - 1) / wpb, nranges), SETUP_TPB, 0, st>>>(
+        jobs, hdr, (const PrimeAux *)aux, 0, tabs, tgt, meta, stats, gm, geoms, ranges, ctrs, rcap);
     return cudaGetLastError();
 }
 

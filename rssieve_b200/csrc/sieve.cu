@@ -25,16 +25,16 @@ __device__ __forceinline__ u32 mod64_32(u64 x, u32 r)
 }
 
 // One CTA sieves odd values base_odd + 2*i for i in [blk*BITS, blk*BITS+nbits).
-// ctrs[0] counts survivors written to cands.
-__global__ void __launch_bounds__(SIEVE_TPB) k_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *__restrict__ sp,
-                                                     u32 nsp, u64 *__restrict__ cands, u32 cand_cap, u32 *ctrs,
-                                                     u32 *err)
+// ctrs[0] counts survivors written to cands.  The caller's exit test is
+// uniform over the CTA.
+__device__ __forceinline__ void sieve_block(u64 base_odd, u64 nodd, u32 blk, const u32 *__restrict__ sp, u32 nsp,
+                                            u64 *__restrict__ cands, u32 cand_cap, u32 *ctrs, u32 *err)
 {
     constexpr u32 BITS = SIEVE_WORDS * 32;
     __shared__ u32 bits[SIEVE_WORDS];
     __shared__ u32 starts[7000];
     const u32 tid = threadIdx.x;
-    const u64 i0 = (u64)blockIdx.x * BITS;
+    const u64 i0 = (u64)blk * BITS;
     if (i0 >= nodd) return;
     const u32 nbits = (u32)min((u64)BITS, nodd - i0);
     const u64 bb = base_odd + 2 * i0;                   // value of bit 0 (odd)
@@ -117,6 +117,23 @@ __global__ void __launch_bounds__(SIEVE_TPB) k_sieve(u64 base_odd, u64 nodd, u64
     }
 }
 
+__global__ void __launch_bounds__(SIEVE_TPB) k_sieve(u64 base_odd, u64 nodd, const u32 *__restrict__ sp, u32 nsp,
+                                                     u64 *__restrict__ cands, u32 cand_cap, u32 *ctrs, u32 *err)
+{
+    sieve_block(base_odd, nodd, blockIdx.x, sp, nsp, cands, cand_cap, ctrs, err);
+}
+
+// Batch round: blockIdx.y is the range; its window and buffers come from the
+// range's slots.
+__global__ void __launch_bounds__(SIEVE_TPB) k_sieve_batch(const BatchWin *__restrict__ wins, const u32 *__restrict__ sp,
+                                                           u32 nsp, u64 *__restrict__ cands, u32 ccap, u32 *ctrs,
+                                                           u32 *err)
+{
+    const u32 r = blockIdx.y;
+    const BatchWin w = wins[r];
+    sieve_block(w.base_odd, w.nodd, blockIdx.x, sp, nsp, cands + (size_t)r * ccap, ccap, ctrs + r * BR_CTRS, err);
+}
+
 // Deterministic primality below 2^64: the seven strong-probable-prime bases
 // of verify_factor.c:102.
 __device__ bool is_prime_mr(u64 n)
@@ -142,11 +159,11 @@ __device__ bool is_prime_mr(u64 n)
     return true;
 }
 
-__global__ void __launch_bounds__(256) k_mr(const u64 *__restrict__ cands, const u32 *__restrict__ ctrs,
-                                            u32 cand_cap, u64 *__restrict__ primes, u32 prime_cap, u32 *prime_ctr,
-                                            u32 *err)
+// Warp-stride Miller-Rabin over cands[0, min(*cand_ctr, cand_cap)) with ballot compaction into primes.
+__device__ __forceinline__ void mr_list(const u64 *__restrict__ cands, const u32 *cand_ctr, u32 cand_cap,
+                                        u64 *__restrict__ primes, u32 prime_cap, u32 *prime_ctr, u32 *err)
 {
-    const u32 n = min(ctrs[0], cand_cap);
+    const u32 n = min(*cand_ctr, cand_cap);
     const u32 lane = threadIdx.x & 31;
     const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -171,13 +188,77 @@ __global__ void __launch_bounds__(256) k_mr(const u64 *__restrict__ cands, const
     }
 }
 
+__global__ void __launch_bounds__(256) k_mr(const u64 *__restrict__ cands, const u32 *__restrict__ ctrs,
+                                            u32 cand_cap, u64 *__restrict__ primes, u32 prime_cap, u32 *prime_ctr,
+                                            u32 *err)
+{
+    mr_list(cands, ctrs, cand_cap, primes, prime_cap, prime_ctr, err);
+}
+
+// Batch round: blockIdx.y is the range.
+__global__ void __launch_bounds__(256) k_mr_batch(const u64 *__restrict__ cands, u32 ccap, u64 *__restrict__ primes,
+                                                  u32 rcap, u32 *ctrs, u32 *err)
+{
+    const u32 r = blockIdx.y;
+    mr_list(cands + (size_t)r * ccap, ctrs + r * BR_CTRS, ccap, primes + (size_t)r * rcap, rcap,
+            ctrs + r * BR_CTRS + 1, err);
+}
+
+// Next window of every range, sized for about 0.6*rcap primes (width
+// 0.6*rcap*ln p) and clamped to the range's end (a range lies entirely on one
+// side of 2^63).  Also clears the range's counters.
+__global__ void k_batch_windows(BatchRange *ranges, BatchWin *wins, u32 nranges, u32 rcap, u32 *ctrs)
+{
+    const u32 r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nranges) return;
+    BatchRange R = ranges[r];
+    BatchWin w;
+    w.lo = R.p_cur;
+    w.hi = R.p_cur;
+    if (R.p_cur < R.p_end) {
+        const double lnp = log((double)(R.p_cur < 3 ? 3 : R.p_cur));
+        u64 width = (u64)(0.6 * (double)rcap * lnp);
+        if (width < 65536) width = 65536;
+        w.hi = (R.p_end - R.p_cur > width) ? R.p_cur + width : R.p_end;
+    }
+    u64 lo = w.lo < 3 ? 3 : w.lo;
+    w.base_odd = lo | 1ull;
+    w.nodd = (w.hi > w.base_odd) ? (w.hi - w.base_odd + 1) / 2 : 0;
+    wins[r] = w;
+    ranges[r].p_cur = w.hi;
+    for (int i = 0; i < BR_CTRS; ++i) ctrs[r * BR_CTRS + i] = 0;
+}
+
 cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp, u64 *cands, u32 cand_cap, u32 *ctrs,
                          u32 *err, cudaStream_t st)
 {
+    (void)hi;
     if (nodd == 0) return cudaSuccess;
     constexpr u64 BITS = (u64)SIEVE_WORDS * 32;
     u64 blocks = (nodd + BITS - 1) / BITS;
-    k_sieve<<<(unsigned)blocks, SIEVE_TPB, 0, st>>>(base_odd, nodd, hi, sp, nsp, cands, cand_cap, ctrs, err);
+    k_sieve<<<(unsigned)blocks, SIEVE_TPB, 0, st>>>(base_odd, nodd, sp, nsp, cands, cand_cap, ctrs, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_windows(BatchRange *ranges, BatchWin *wins, u32 nranges, u32 rcap, u32 *ctrs, cudaStream_t st)
+{
+    k_batch_windows<<<(nranges + 127) / 128, 128, 0, st>>>(ranges, wins, nranges, rcap, ctrs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sieve_batch(const BatchWin *wins, u32 nranges, u32 max_blocks, const u32 *sp, u32 nsp, u64 *cands,
+                               u32 ccap, u32 *ctrs, u32 *err, cudaStream_t st)
+{
+    k_sieve_batch<<<dim3(max_blocks, nranges), SIEVE_TPB, 0, st>>>(wins, sp, nsp, cands, ccap, ctrs, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges, u32 *err,
+                            int sms, cudaStream_t st)
+{
+    unsigned bx = (unsigned)((sms * 8 + nranges - 1) / nranges);
+    if (bx < 2) bx = 2;
+    k_mr_batch<<<dim3(bx, nranges), 256, 0, st>>>(cands, ccap, primes, rcap, ctrs, err);
     return cudaGetLastError();
 }
 
