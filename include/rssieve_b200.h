@@ -34,6 +34,7 @@ extern "C" {
 #define RS_ESTATE (-7)          /* checkpoint missing, corrupt or for another job */
 #define RS_EVERIFY (-8)         /* a device factor failed host verification */
 #define RS_ENODEV (-9)          /* no CUDA device / library built without one */
+#define RS_EBUSY (-10)          /* no free batch slot: run rounds and release finished jobs */
 
 /* One job: up to 100 sequences sharing a base and an n-range.  Mirrors the
  * job fields of workStatus (cl_sieve.h:21-26) plus the candidate bitmap of
@@ -182,19 +183,33 @@ int rs_last_timing(rs_ctx *ctx, double *bsgs_ms, double *total_kernel_ms, uint32
  * unfinished job sieves its next window (about 39 000 primes) per round, the
  * BSGS work of all jobs that share a geometry runs in one persistent launch,
  * and the host waits once per round.  After the first round a round is
- * replayed from a captured CUDA graph.  Each job's eliminated terms equal what
- * rs_run_range gives for the same job and p-range. */
+ * replayed from a captured CUDA graph.  Jobs may be added between rounds and
+ * released when done, so a batch also serves a stream of work units.  Each
+ * job's eliminated terms equal what rs_run_range gives for the same job and
+ * p-range. */
 typedef struct rs_batch rs_batch;
-int rs_batch_create(int device, rs_batch **out);
+/* max_jobs job slots and range_slots range slots (0: 64 each).  Each range slot
+ * holds one round's buffers (about 136 MB); a job takes one range slot, or two
+ * when its p-range straddles 2^63. */
+int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slots, rs_batch **out);
 void rs_batch_destroy(rs_batch *b);
 /* A caller stream (cudaStream_t as void*, not the legacy NULL stream); only
  * before the first rs_batch_run. */
 int rs_batch_set_stream(rs_batch *b, void *stream);
-/* Adds a job with its p-range [p0, p1) (3 <= p0 < p1); q fixes its baby-step
+/* Adds a job with its p-range [p0, p1) (3 <= p0 < p1, or p0 == p1 for a
+ * template, see rs_batch_add_clone); q fixes its baby-step
  * count (as rs_set_baby_steps) or 0 takes the cost model's choice.  The job's
- * bitmap is copied.  *job (may be NULL) receives its index.  Only before the
- * first rs_batch_run. */
+ * bitmap is copied to the device.  *job (may be NULL) receives its slot.
+ * RS_EBUSY when no job or range slot is free. */
 int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t p1, uint32_t q, uint32_t *job);
+/* A new job with job src's sequences, geometry and current bitmap, copied on
+ * the device (no host transfer), over [p0, p1).  A job added with p0 == p1 is
+ * a resident template: it takes no range slot and never runs, and serves as
+ * the source of clones -- e.g. one template per input file, one clone per
+ * work unit, each unit with its own bitmap. */
+int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64_t p1, uint32_t *job);
+/* Frees a job's slots (fetch its factors and bitmap first). */
+int rs_batch_release(rs_batch *b, uint32_t job);
 /* Runs up to max_rounds rounds (0: until every job is done); *done = 1 once
  * every job's p-range is finished. */
 int rs_batch_run(rs_batch *b, uint32_t max_rounds, int *done);
@@ -204,7 +219,7 @@ int rs_batch_bitmap_download(rs_batch *b, uint32_t job, uint32_t *dst, size_t wo
 /* A job's baby-step count, primes tested so far and whether its range is done
  * (each pointer may be NULL). */
 int rs_batch_job_info(rs_batch *b, uint32_t job, uint32_t *q, uint64_t *primes, int *done);
-/* Counters summed over the batch's jobs. */
+/* Counters summed over every job the batch has run. */
 int rs_batch_counters(rs_batch *b, rs_counters *out);
 
 /* Throughput of independent 64-bit Montgomery products (the kernels' mmul)

@@ -16,8 +16,8 @@ LIB_PATH = os.path.join(PKG, "_lib", "librssieve_b200.so")
 CLI_PATH = os.path.join(PKG, "_lib", "rssieve")
 MAX_SEQ = 100
 
-RS_OK, RS_EARG, RS_ECUDA, RS_ENOMEM, RS_EDEVICE, RS_EIO, RS_EPARSE, RS_ESTATE, RS_EVERIFY, RS_ENODEV = (
-    0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
+RS_OK, RS_EARG, RS_ECUDA, RS_ENOMEM, RS_EDEVICE, RS_EIO, RS_EPARSE, RS_ESTATE, RS_EVERIFY, RS_ENODEV, RS_EBUSY = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8, -9, -10)
 
 FACTOR_DT = np.dtype([("p", "<u8"), ("n", "<u4"), ("seq", "<u4")])
 COUNTER_FIELDS = ("primes", "skipped", "full", "parity", "targets", "baby", "giant", "small_order",
@@ -52,7 +52,7 @@ EXPORTS = (
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
     "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_primes_generate_noalloc",
     "rs_set_baby_steps", "rs_get_baby_steps",
-    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_run",
+    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone", "rs_batch_release", "rs_batch_run",
     "rs_batch_factors_fetch", "rs_batch_bitmap_download", "rs_batch_job_info", "rs_batch_counters",
 )
 BABY_STEPS = (1024, 2048, 4096, 8192, 16384)   # accepted by rs_set_baby_steps (0: automatic)
@@ -105,7 +105,9 @@ def lib():
         "rs_mulmod_peak": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "rs_primes_generate_noalloc": (C.c_int, [u64, u64, vp, u32, vp, vp]),
         "rs_set_baby_steps": (C.c_int, [vp, u32]),
-        "rs_batch_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+        "rs_batch_create": (C.c_int, [C.c_int, u32, u32, C.POINTER(vp)]),
+        "rs_batch_release": (C.c_int, [vp, u32]),
+        "rs_batch_add_clone": (C.c_int, [vp, u32, u64, u64, C.POINTER(u32)]),
         "rs_batch_destroy": (None, [vp]),
         "rs_batch_set_stream": (C.c_int, [vp, vp]),
         "rs_batch_add": (C.c_int, [vp, PS, u64, u64, u32, C.POINTER(u32)]),
@@ -354,11 +356,11 @@ class Sieve:
 class Batch:
     """Many independent jobs sieved together on one device (rs_batch_*)."""
 
-    def __init__(self, device=0):
+    def __init__(self, device=0, max_jobs=0, range_slots=0):
         L = lib()
         self._b = C.c_void_p()
-        _check(L.rs_batch_create(device, C.byref(self._b)), "rs_batch_create")
-        self._seqs = []
+        _check(L.rs_batch_create(device, max_jobs, range_slots, C.byref(self._b)), "rs_batch_create")
+        self._seqs = {}
 
     def close(self):
         if getattr(self, "_b", None) and self._b.value:
@@ -372,11 +374,28 @@ class Batch:
             pass
 
     def add(self, seqs, p0, p1, q=0):
-        """Add a job over [p0, p1); returns its index."""
+        """Add a job over [p0, p1); returns its slot, or None when no slot is free."""
         j = C.c_uint32(0)
-        _check(lib().rs_batch_add(self._b, seqs._p, p0, p1, q, C.byref(j)), "rs_batch_add")
-        self._seqs.append(seqs)
+        rc = lib().rs_batch_add(self._b, seqs._p, p0, p1, q, C.byref(j))
+        if rc == RS_EBUSY:
+            return None
+        _check(rc, "rs_batch_add")
+        self._seqs[j.value] = seqs
         return j.value
+
+    def add_clone(self, src, p0, p1):
+        """A job copying slot src's sequences and bitmap on the device; None when no slot is free."""
+        j = C.c_uint32(0)
+        rc = lib().rs_batch_add_clone(self._b, src, p0, p1, C.byref(j))
+        if rc in (RS_EBUSY, RS_ENOMEM):
+            return None
+        _check(rc, "rs_batch_add_clone")
+        self._seqs[j.value] = self._seqs[src]
+        return j.value
+
+    def release(self, job):
+        _check(lib().rs_batch_release(self._b, job), "rs_batch_release")
+        self._seqs.pop(job, None)
 
     def run(self, max_rounds=0):
         """Run up to max_rounds rounds (0: to completion); True once every job is done."""

@@ -24,6 +24,16 @@
 // Montgomery above) that share its bitmap and factor list.  Each job's BSGS
 // geometry comes from the per-prime cost model (geom_model_best) unless the
 // caller fixes Q.
+//
+// Capacity is fixed when the batch is created: job slots and range slots (each
+// range slot owns one round's buffers, about 136 MB).  Jobs can be added
+// between rounds -- their tables are written to device memory that the
+// captured round reads -- and a finished job's slots are released for the
+// next one, so the batch also serves a stream of arriving work units.  The
+// ten BSGS groups (geometry x product) cover every range slot and count only
+// the slots currently in them, so the captured round never changes.  A job's
+// bitmap and factor list come from the stream-ordered allocator, so admitting
+// or releasing a job does not synchronise the device.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -37,10 +47,12 @@ namespace {
 
 constexpr u32 RCAP = 1u << 16;     // primes per range per round
 constexpr u32 CCAP = 2 * RCAP;     // sieve survivors per range per round (at most ~1.3 RCAP)
+constexpr u32 DEF_JOBS = 64, DEF_RANGES = 64;
 
 struct BJob {
+    bool used = false;
     JobDev jd;
-    int geom;
+    int geom = 0;
     u32 *d_bitmap = nullptr;
     size_t bitmap_words = 0;
     FactorRec *d_factors = nullptr;
@@ -51,9 +63,7 @@ struct BJob {
 struct Group {
     int geom;
     bool shoup;
-    std::vector<u32> ranges;
-    u32 *d_ranges = nullptr;   // the group's range indices
-    u32 *d_prefix = nullptr;   // nr + 1 prefix sums of their prime counts
+    u32 *d_prefix = nullptr;   // nr + 1 prefix sums of the group's prime counts
     u32 *d_work = nullptr;     // work counter of the group's BSGS launch
 };
 
@@ -62,10 +72,12 @@ __global__ void k_batch_account(const BatchRange *ranges, const u32 *ctrs, u32 r
 {
     const u32 r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nranges) return;
+    const BatchRange R = ranges[r];
+    if (!R.active) return;
     const u32 n = min(ctrs[r * BR_CTRS + 1], rcap);
     range_primes[r] += n;
     if (n) atomicAdd((unsigned long long *)&stats[ST_PRIMES], (unsigned long long)n);
-    if (ranges[r].p_cur < ranges[r].p_end) atomicAdd(unfinished, 1u);
+    if (R.p_cur < R.p_end) atomicAdd(unfinished, 1u);
 }
 
 }  // namespace
@@ -73,11 +85,12 @@ __global__ void k_batch_account(const BatchRange *ranges, const u32 *ctrs, u32 r
 struct rs_batch {
     int device = -1;
     int sms = 0;
+    u32 max_jobs = 0, nranges = 0;
     cudaStream_t own = nullptr, stream = nullptr;
     std::vector<BJob> jobs;
-    std::vector<BatchRange> h_ranges;
+    std::vector<BatchRange> h_ranges;      // host copy of the range slots' fixed fields
+    std::vector<char> range_used;
     std::vector<Group> groups;
-    bool built = false;
     // device tables
     u32 *d_sp = nullptr;
     u32 nsp = 0;
@@ -98,7 +111,7 @@ struct rs_batch {
     u32 *d_err = nullptr;
     u64 *d_stats = nullptr;
     u32 *d_unfinished = nullptr;
-    u32 *h_pin = nullptr;       // [0] error word, [1] unfinished ranges
+    u32 *h_pin = nullptr;       // [0] error word, [1] unfinished ranges, [2] factor count
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     u64 rounds = 0;
@@ -118,14 +131,15 @@ extern "C" void rs_batch_destroy(rs_batch *b)
 {
     if (!b) return;
     if (b->device >= 0) cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     for (auto &j : b->jobs) {
-        cudaFree(j.d_bitmap);
-        cudaFree(j.d_factors);
+        if (j.d_bitmap) cudaFreeAsync(j.d_bitmap, b->stream);
+        if (j.d_factors) cudaFreeAsync(j.d_factors, b->stream);
     }
+    if (b->stream) cudaStreamSynchronize(b->stream);
     for (auto &g : b->groups) {
-        cudaFree(g.d_ranges);
         cudaFree(g.d_prefix);
         cudaFree(g.d_work);
     }
@@ -138,10 +152,16 @@ extern "C" void rs_batch_destroy(rs_batch *b)
     delete b;
 }
 
-extern "C" int rs_batch_create(int device, rs_batch **out)
+extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slots, rs_batch **out)
 {
     if (!out) return RS_EARG;
     *out = nullptr;
+    if (max_jobs == 0) max_jobs = DEF_JOBS;
+    if (range_slots == 0) range_slots = DEF_RANGES;
+    if (max_jobs > 65536 || range_slots > 4096) {
+        rs_set_error("rs_batch_create: at most 65536 jobs and 4096 range slots");
+        return RS_EARG;
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         rs_set_error("no CUDA device available");
@@ -153,103 +173,23 @@ extern "C" int rs_batch_create(int device, rs_batch **out)
     }
     rs_batch *b = new rs_batch();
     b->device = device;
+    b->max_jobs = max_jobs;
+    b->nranges = range_slots;
     auto fail = [&](int rc) { rs_batch_destroy(b); return rc; };
     if (cudaSetDevice(device) != cudaSuccess) return fail(RS_ECUDA);
     if (cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return fail(RS_ECUDA);
     if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess) return fail(RS_ECUDA);
     b->stream = b->own;
+    b->jobs.resize(max_jobs);
+    b->h_ranges.assign(range_slots, BatchRange{});
+    b->range_used.assign(range_slots, 0);
+    const u32 J = max_jobs, R = range_slots;
     std::vector<u32> sp = rs_small_primes();
     b->nsp = (u32)sp.size();
-    if (cudaMalloc(&b->d_sp, sp.size() * 4) != cudaSuccess || cudaMalloc(&b->d_err, 4) != cudaSuccess ||
-        cudaMalloc(&b->d_stats, ST_COUNT * 8) != cudaSuccess || cudaMalloc(&b->d_unfinished, 4) != cudaSuccess ||
-        cudaMallocHost(&b->h_pin, 16) != cudaSuccess) {
-        rs_set_error("device allocation failed");
-        return fail(RS_ENOMEM);
-    }
-    if (cudaMemcpy(b->d_sp, sp.data(), sp.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(b->d_err, 0, 4) != cudaSuccess || cudaMemset(b->d_stats, 0, ST_COUNT * 8) != cudaSuccess)
-        return fail(RS_ECUDA);
-    if (bsgs_prepare() != cudaSuccess) {
-        rs_set_error("cannot configure the BSGS kernels' shared memory");
-        return fail(RS_ECUDA);
-    }
-    *out = b;
-    return RS_OK;
-}
-
-extern "C" int rs_batch_set_stream(rs_batch *b, void *stream)
-{
-    if (!b || b->built) return RS_EARG;      // the captured round is bound to one stream
-    b->stream = stream ? (cudaStream_t)stream : b->own;
-    return RS_OK;
-}
-
-extern "C" int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t p1, uint32_t q, uint32_t *job)
-{
-    if (!b || !s) return RS_EARG;
-    if (b->built) {
-        rs_set_error("rs_batch_add: the batch has already run; create a new batch for more jobs");
-        return RS_EARG;
-    }
-    if (q != 0 && geom_index(q) < 0) {
-        rs_set_error("baby-step count %u is not one of 1024, 2048, 4096, 8192, 16384 (or 0 for the model)", q);
-        return RS_EARG;
-    }
-    int rc = rs_seqs_validate(s);
-    if (rc) return rc;
-    if (p0 < 3) p0 = 3;
-    if (p1 <= p0) {
-        rs_set_error("rs_batch_add: empty p-range");
-        return RS_EARG;
-    }
-    BCU(cudaSetDevice(b->device));
-    BJob J;
-    jobdev_from_seqs(s, &J.jd);
-    J.geom = q ? geom_index(q) : geom_model_best(J.jd.kcount, J.jd.L);
-    J.bitmap_words = (size_t)s->kcount * s->words_per_seq;
-    const uint64_t cand = rs_seqs_count(s);
-    J.factor_cap = (u32)std::min<uint64_t>(cand + 1, 0xFFFFFFF0ull);
-    if (cudaMalloc(&J.d_bitmap, J.bitmap_words * 4) != cudaSuccess ||
-        cudaMalloc(&J.d_factors, (size_t)J.factor_cap * sizeof(FactorRec)) != cudaSuccess) {
-        cudaFree(J.d_bitmap);
-        cudaFree(J.d_factors);
-        rs_set_error("cannot allocate the bitmap and factor buffer of batch job %zu", b->jobs.size());
-        return RS_ENOMEM;
-    }
-    J.jd.bitmap = J.d_bitmap;
-    BCU(cudaMemcpy(J.d_bitmap, s->bitmap, J.bitmap_words * 4, cudaMemcpyHostToDevice));
-    const u32 jid = (u32)b->jobs.size();
-    const u64 TOP = 1ull << 63;
-    auto add_range = [&](u64 lo, u64 hi) {
-        BatchRange R;
-        R.p_cur = lo;
-        R.p_end = hi;
-        R.job = jid;
-        R.pad_ = 0;
-        J.ranges.push_back((u32)b->h_ranges.size());
-        b->h_ranges.push_back(R);
-    };
-    if (p0 < TOP && p1 > TOP) {
-        add_range(p0, TOP);
-        add_range(TOP, p1);
-    } else {
-        add_range(p0, p1);
-    }
-    b->jobs.push_back(J);
-    if (job) *job = jid;
-    return RS_OK;
-}
-
-// Allocates the round buffers and device tables and forms the BSGS groups.
-static int batch_build(rs_batch *b)
-{
-    const u32 J = (u32)b->jobs.size(), R = (u32)b->h_ranges.size();
-    if (J == 0) {
-        rs_set_error("rs_batch_run: no jobs");
-        return RS_EARG;
-    }
     auto alloc = [&](void **p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess; };
-    if (!alloc((void **)&b->d_jobs, J * sizeof(JobDev)) || !alloc((void **)&b->d_geoms, J * sizeof(JobGeom)) ||
+    if (!alloc((void **)&b->d_sp, sp.size() * 4) || !alloc((void **)&b->d_err, 4) ||
+        !alloc((void **)&b->d_stats, ST_COUNT * 8) || !alloc((void **)&b->d_unfinished, 4) ||
+        !alloc((void **)&b->d_jobs, (size_t)J * sizeof(JobDev)) || !alloc((void **)&b->d_geoms, J * sizeof(JobGeom)) ||
         !alloc((void **)&b->d_args, J * sizeof(BsgsArgs)) || !alloc((void **)&b->d_fctrs, J * 4) ||
         !alloc((void **)&b->d_ranges, R * sizeof(BatchRange)) || !alloc((void **)&b->d_wins, R * sizeof(BatchWin)) ||
         !alloc((void **)&b->d_ctrs, (size_t)R * BR_CTRS * 4) || !alloc((void **)&b->d_range_primes, R * 8) ||
@@ -258,67 +198,198 @@ static int batch_build(rs_batch *b)
         !alloc(&b->d_aux, (size_t)R * RCAP * setup_aux_bytes()) ||
         !alloc((void **)&b->d_tabs, (size_t)R * RCAP * TABS * 8) ||
         !alloc((void **)&b->d_tgt, (size_t)R * RCAP * KSTRIDE * 8) ||
-        !alloc((void **)&b->d_meta, (size_t)R * RCAP * KSTRIDE)) {
-        rs_set_error("cannot allocate the round buffers of %u ranges", R);
+        !alloc((void **)&b->d_meta, (size_t)R * RCAP * KSTRIDE) || cudaMallocHost(&b->h_pin, 16) != cudaSuccess) {
+        rs_set_error("cannot allocate a batch of %u range slots (about %zu MB)", R,
+                     (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 9 + 24 + 8 + 16) >> 20);
+        return fail(RS_ENOMEM);
+    }
+    if (cudaMemcpy(b->d_sp, sp.data(), sp.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b->d_err, 0, 4) != cudaSuccess || cudaMemset(b->d_stats, 0, ST_COUNT * 8) != cudaSuccess ||
+        cudaMemset(b->d_jobs, 0, (size_t)J * sizeof(JobDev)) != cudaSuccess ||
+        cudaMemset(b->d_geoms, 0, J * sizeof(JobGeom)) != cudaSuccess ||
+        cudaMemset(b->d_args, 0, J * sizeof(BsgsArgs)) != cudaSuccess || cudaMemset(b->d_fctrs, 0, J * 4) != cudaSuccess ||
+        cudaMemset(b->d_ranges, 0, R * sizeof(BatchRange)) != cudaSuccess ||
+        cudaMemset(b->d_ctrs, 0, (size_t)R * BR_CTRS * 4) != cudaSuccess ||
+        cudaMemset(b->d_range_primes, 0, R * 8) != cudaSuccess)
+        return fail(RS_ECUDA);
+    if (bsgs_prepare() != cudaSuccess) {
+        rs_set_error("cannot configure the BSGS kernels' shared memory");
+        return fail(RS_ECUDA);
+    }
+    for (int g = 0; g < NGEOM; ++g)
+        for (int m = 0; m < 2; ++m) {
+            Group G{g, m == 1, nullptr, nullptr};
+            if (!alloc((void **)&G.d_prefix, (R + 1) * 4) || !alloc((void **)&G.d_work, 4)) {
+                b->groups.push_back(G);
+                rs_set_error("cannot allocate the BSGS group tables");
+                return fail(RS_ENOMEM);
+            }
+            b->groups.push_back(G);
+        }
+    *out = b;
+    return RS_OK;
+}
+
+extern "C" int rs_batch_set_stream(rs_batch *b, void *stream)
+{
+    if (!b || b->rounds) return RS_EARG;     // the captured round is bound to one stream
+    if (!stream) {
+        rs_set_error("rs_batch_set_stream: a batch captures its rounds, which the legacy NULL stream cannot");
+        return RS_EARG;
+    }
+    b->stream = (cudaStream_t)stream;
+    return RS_OK;
+}
+
+static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_t p0, uint64_t p1, uint32_t q,
+                         uint32_t *job);
+
+extern "C" int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t p1, uint32_t q, uint32_t *job)
+{
+    if (!b || !s) return RS_EARG;
+    if (q != 0 && geom_index(q) < 0) {
+        rs_set_error("baby-step count %u is not one of 1024, 2048, 4096, 8192, 16384 (or 0 for the model)", q);
+        return RS_EARG;
+    }
+    int rc = rs_seqs_validate(s);
+    if (rc) return rc;
+    if (p1 < p0) {
+        rs_set_error("rs_batch_add: p1 < p0");
+        return RS_EARG;
+    }
+    return batch_add_job(b, s, nullptr, p0, p1, q, job);
+}
+
+// Adds a job from host sequences s, or (s == nullptr) as a copy of job slot src
+// made on the device.  p0 == p1: a resident template that takes no range slot.
+static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_t p0, uint64_t p1, uint32_t q,
+                         uint32_t *job)
+{
+    const bool tmpl = (p0 == p1);
+    if (p0 < 3) p0 = 3;
+    if (!tmpl && p1 <= p0) {
+        rs_set_error("rs_batch_add: empty p-range");
+        return RS_EARG;
+    }
+    const u64 TOP = 1ull << 63;
+    const u32 need = tmpl ? 0 : (p0 < TOP && p1 > TOP) ? 2 : 1;
+    u32 jid = 0;
+    while (jid < b->max_jobs && b->jobs[jid].used) ++jid;
+    std::vector<u32> slots;
+    for (u32 r = 0; r < b->nranges && slots.size() < need; ++r)
+        if (!b->range_used[r]) slots.push_back(r);
+    if (jid == b->max_jobs || slots.size() < need) {
+        rs_set_error("rs_batch_add: no free job or range slot (%u jobs, %u range slots)", b->max_jobs, b->nranges);
+        return RS_EBUSY;
+    }
+    BCU(cudaSetDevice(b->device));
+    BJob &J = b->jobs[jid];
+    J = BJob();
+    if (s) {
+        jobdev_from_seqs(s, &J.jd);
+        J.geom = q ? geom_index(q) : geom_model_best(J.jd.kcount, J.jd.L);
+        J.bitmap_words = (size_t)s->kcount * s->words_per_seq;
+        const uint64_t cand = rs_seqs_count(s);
+        J.factor_cap = (u32)std::min<uint64_t>(cand + 1, 0xFFFFFFF0ull);
+    } else {
+        J.jd = src->jd;
+        J.geom = src->geom;
+        J.bitmap_words = src->bitmap_words;
+        J.factor_cap = src->factor_cap;
+    }
+    const u32 fcap = tmpl ? 1u : J.factor_cap;       // a template never claims; its clones get factor_cap
+    if (cudaMallocAsync((void **)&J.d_bitmap, J.bitmap_words * 4, b->stream) != cudaSuccess ||
+        cudaMallocAsync((void **)&J.d_factors, (size_t)fcap * sizeof(FactorRec), b->stream) != cudaSuccess) {
+        if (J.d_bitmap) cudaFreeAsync(J.d_bitmap, b->stream);
+        if (J.d_factors) cudaFreeAsync(J.d_factors, b->stream);
+        J = BJob();
+        rs_set_error("cannot allocate the bitmap and factor buffer of a batch job");
         return RS_ENOMEM;
     }
-    std::vector<JobDev> jd(J);
-    std::vector<JobGeom> jg(J);
-    std::vector<BsgsArgs> ja(J);
-    for (u32 j = 0; j < J; ++j) {
-        const BJob &B = b->jobs[j];
-        const BsgsGeom &g = BSGS_GEOMS[B.geom];
-        jd[j] = B.jd;
-        JobGeom &G = jg[j];
-        G.q = g.q; G.c = g.c; G.tpb = g.tpb; G.pad_ = 0;
-        G.m1 = (u32)(((u64)B.jd.L + g.q - 1) / g.q);
-        G.m2 = (u32)(((u64)B.jd.L + 2ull * g.q - 1) / (2ull * g.q));
-        BsgsArgs &A = ja[j];
-        A.base = B.jd.base; A.nmin = B.jd.nmin; A.nmax = B.jd.nmax; A.words = B.jd.words;
-        A.M1 = G.m1; A.M2 = G.m2;
-        A.bitmap = B.d_bitmap;
-        A.factors = B.d_factors;
-        A.factor_ctr = b->d_fctrs + j;
-        A.factor_cap = B.factor_cap;
-        A.stats = b->d_stats;
-        A.err = b->d_err;
+    J.jd.bitmap = J.d_bitmap;
+    J.used = true;
+    const BsgsGeom &g = BSGS_GEOMS[J.geom];
+    JobGeom G;
+    G.q = g.q; G.c = g.c; G.tpb = g.tpb; G.pad_ = 0;
+    G.m1 = (u32)(((u64)J.jd.L + g.q - 1) / g.q);
+    G.m2 = (u32)(((u64)J.jd.L + 2ull * g.q - 1) / (2ull * g.q));
+    BsgsArgs A;
+    memset(&A, 0, sizeof A);
+    A.base = J.jd.base; A.nmin = J.jd.nmin; A.nmax = J.jd.nmax; A.words = J.jd.words;
+    A.M1 = G.m1; A.M2 = G.m2;
+    A.bitmap = J.d_bitmap;
+    A.factors = J.d_factors;
+    A.factor_ctr = b->d_fctrs + jid;
+    A.factor_cap = fcap;
+    A.stats = b->d_stats;
+    A.err = b->d_err;
+    if (s)    // pageable source: the copy completes before the call returns
+        BCU(cudaMemcpyAsync(J.d_bitmap, s->bitmap, J.bitmap_words * 4, cudaMemcpyHostToDevice, b->stream));
+    else
+        BCU(cudaMemcpyAsync(J.d_bitmap, src->d_bitmap, J.bitmap_words * 4, cudaMemcpyDeviceToDevice, b->stream));
+    BCU(cudaMemcpyAsync(b->d_jobs + jid, &J.jd, sizeof(JobDev), cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaMemcpyAsync(b->d_geoms + jid, &G, sizeof G, cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaMemcpyAsync(b->d_args + jid, &A, sizeof A, cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaMemsetAsync(b->d_fctrs + jid, 0, 4, b->stream));
+    u64 lo = p0;
+    for (u32 i = 0; i < need; ++i) {
+        const u32 r = slots[i];
+        const u64 hi = (need == 2 && i == 0) ? TOP : p1;
+        BatchRange R;
+        memset(&R, 0, sizeof R);
+        R.p_cur = lo;
+        R.p_end = hi;
+        R.job = jid;
+        R.active = 1;
+        R.shoup = (hi <= TOP) ? 1 : 0;
+        R.geom = (u8)J.geom;
+        b->h_ranges[r] = R;
+        b->range_used[r] = 1;
+        J.ranges.push_back(r);
+        BCU(cudaMemcpyAsync(b->d_ranges + r, &b->h_ranges[r], sizeof R, cudaMemcpyHostToDevice, b->stream));
+        BCU(cudaMemsetAsync(b->d_range_primes + r, 0, 8, b->stream));
+        lo = hi;
     }
-    BCU(cudaMemcpy(b->d_jobs, jd.data(), J * sizeof(JobDev), cudaMemcpyHostToDevice));
-    BCU(cudaMemcpy(b->d_geoms, jg.data(), J * sizeof(JobGeom), cudaMemcpyHostToDevice));
-    BCU(cudaMemcpy(b->d_args, ja.data(), J * sizeof(BsgsArgs), cudaMemcpyHostToDevice));
-    BCU(cudaMemcpy(b->d_ranges, b->h_ranges.data(), R * sizeof(BatchRange), cudaMemcpyHostToDevice));
-    BCU(cudaMemset(b->d_fctrs, 0, J * 4));
-    BCU(cudaMemset(b->d_range_primes, 0, R * 8));
-    BCU(cudaMemset(b->d_ctrs, 0, (size_t)R * BR_CTRS * 4));
-    // groups: ranges with the same geometry and the same side of 2^63
-    for (u32 r = 0; r < R; ++r) {
-        const int g = b->jobs[b->h_ranges[r].job].geom;
-        const bool shoup = b->h_ranges[r].p_end <= (1ull << 63);
-        auto it = std::find_if(b->groups.begin(), b->groups.end(),
-                               [&](const Group &x) { return x.geom == g && x.shoup == shoup; });
-        if (it == b->groups.end()) {
-            b->groups.push_back(Group{g, shoup, {}, nullptr, nullptr, nullptr});
-            it = b->groups.end() - 1;
-        }
-        it->ranges.push_back(r);
-    }
-    for (auto &g : b->groups) {
-        const u32 nr = (u32)g.ranges.size();
-        if (!alloc((void **)&g.d_ranges, nr * 4) || !alloc((void **)&g.d_prefix, (nr + 1) * 4) ||
-            !alloc((void **)&g.d_work, 4)) {
-            rs_set_error("cannot allocate the BSGS group tables");
-            return RS_ENOMEM;
-        }
-        BCU(cudaMemcpy(g.d_ranges, g.ranges.data(), nr * 4, cudaMemcpyHostToDevice));
-    }
-    b->built = true;
+    BCU(cudaStreamSynchronize(b->stream));     // the host structs above go out of scope
+    b->done = false;
+    if (job) *job = jid;
     return RS_OK;
+}
+
+extern "C" int rs_batch_release(rs_batch *b, uint32_t job)
+{
+    if (!b || job >= b->max_jobs || !b->jobs[job].used) return RS_EARG;
+    BCU(cudaSetDevice(b->device));
+    BJob &J = b->jobs[job];
+    for (u32 r : J.ranges) {
+        BatchRange R;
+        memset(&R, 0, sizeof R);
+        b->h_ranges[r] = R;
+        b->range_used[r] = 0;
+        BCU(cudaMemcpyAsync(b->d_ranges + r, &b->h_ranges[r], sizeof R, cudaMemcpyHostToDevice, b->stream));
+    }
+    BCU(cudaFreeAsync(J.d_bitmap, b->stream));
+    BCU(cudaFreeAsync(J.d_factors, b->stream));
+    BCU(cudaStreamSynchronize(b->stream));
+    J = BJob();
+    return RS_OK;
+}
+
+extern "C" int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64_t p1, uint32_t *job)
+{
+    if (!b || src >= b->max_jobs || !b->jobs[src].used) return RS_EARG;
+    if (p1 <= p0 || p1 <= 3) {
+        rs_set_error("rs_batch_add_clone: empty p-range");
+        return RS_EARG;
+    }
+    const BJob copy = b->jobs[src];          // the slot vector is not resized, but keep a stable copy
+    return batch_add_job(b, nullptr, &copy, p0, p1, 0, job);
 }
 
 // Enqueues one round on b->stream (also what the graph captures).
 static int batch_round(rs_batch *b)
 {
-    const u32 R = (u32)b->h_ranges.size();
+    const u32 R = b->nranges;
     cudaStream_t st = b->stream;
     // widest window: 0.6*RCAP*ln(2^64) values, i.e. 0.3*RCAP*44.4 odd values
     const u32 max_blocks = (u32)((0.3 * RCAP * 44.4) / (SIEVE_WORDS * 32.0)) + 2;
@@ -333,11 +404,10 @@ static int batch_round(rs_batch *b)
     a.stats = b->d_stats;
     a.err = b->d_err;
     for (auto &g : b->groups) {
-        const u32 nr = (u32)g.ranges.size();
-        BCU(launch_batch_prefix(g.d_ranges, nr, b->d_ctrs, RCAP, g.d_prefix, st));
+        BCU(launch_batch_prefix(b->d_ranges, R, g.geom, g.shoup, b->d_ctrs, RCAP, g.d_prefix, st));
         BCU(cudaMemsetAsync(g.d_work, 0, 4, st));
-        BCU(launch_bsgs_batch(a, b->d_args, b->d_hdr, b->d_tabs, b->d_tgt, b->d_meta, g.d_ranges, nr, g.d_prefix, RCAP,
-                              g.d_work, g.shoup, g.geom, b->sms, st));
+        BCU(launch_bsgs_batch(a, b->d_args, b->d_hdr, b->d_tabs, b->d_tgt, b->d_meta, R, g.d_prefix, RCAP, g.d_work,
+                              g.shoup, g.geom, b->sms, st));
     }
     k_batch_account<<<(R + 127) / 128, 128, 0, st>>>(b->d_ranges, b->d_ctrs, RCAP, R, b->d_range_primes, b->d_stats,
                                                      b->d_unfinished);
@@ -349,10 +419,9 @@ extern "C" int rs_batch_run(rs_batch *b, uint32_t max_rounds, int *done)
 {
     if (!b) return RS_EARG;
     BCU(cudaSetDevice(b->device));
-    if (!b->built) {
-        int rc = batch_build(b);
-        if (rc) return rc;
-    }
+    bool any = false;
+    for (char u : b->range_used) any = any || u;
+    if (!any) b->done = true;
     for (uint32_t i = 0; (max_rounds == 0 || i < max_rounds) && !b->done; ++i) {
         if (b->rounds == 0) {
             int rc = batch_round(b);                 // eager: sizes the persistent grids
@@ -389,7 +458,7 @@ extern "C" int rs_batch_run(rs_batch *b, uint32_t max_rounds, int *done)
 
 extern "C" int rs_batch_factors_fetch(rs_batch *b, uint32_t job, rs_factor *buf, size_t cap, size_t *n)
 {
-    if (!b || !n || job >= b->jobs.size() || !b->built) return RS_EARG;
+    if (!b || !n || job >= b->max_jobs || !b->jobs[job].used) return RS_EARG;
     BCU(cudaSetDevice(b->device));
     BCU(cudaMemcpyAsync(b->h_pin + 2, b->d_fctrs + job, 4, cudaMemcpyDeviceToHost, b->stream));
     BCU(cudaStreamSynchronize(b->stream));
@@ -410,7 +479,7 @@ extern "C" int rs_batch_factors_fetch(rs_batch *b, uint32_t job, rs_factor *buf,
 
 extern "C" int rs_batch_bitmap_download(rs_batch *b, uint32_t job, uint32_t *dst, size_t words)
 {
-    if (!b || !dst || job >= b->jobs.size() || words < b->jobs[job].bitmap_words) return RS_EARG;
+    if (!b || !dst || job >= b->max_jobs || !b->jobs[job].used || words < b->jobs[job].bitmap_words) return RS_EARG;
     BCU(cudaSetDevice(b->device));
     BCU(cudaMemcpyAsync(dst, b->jobs[job].d_bitmap, b->jobs[job].bitmap_words * 4, cudaMemcpyDeviceToHost, b->stream));
     BCU(cudaStreamSynchronize(b->stream));
@@ -419,26 +488,21 @@ extern "C" int rs_batch_bitmap_download(rs_batch *b, uint32_t job, uint32_t *dst
 
 extern "C" int rs_batch_job_info(rs_batch *b, uint32_t job, uint32_t *q, uint64_t *primes, int *done)
 {
-    if (!b || job >= b->jobs.size()) return RS_EARG;
+    if (!b || job >= b->max_jobs || !b->jobs[job].used) return RS_EARG;
     const BJob &J = b->jobs[job];
     if (q) *q = BSGS_GEOMS[J.geom].q;
     if (!primes && !done) return RS_OK;
-    if (!b->built) {
-        if (primes) *primes = 0;
-        if (done) *done = 0;
-        return RS_OK;
-    }
     BCU(cudaSetDevice(b->device));
-    std::vector<u64> rp(b->h_ranges.size());
-    std::vector<BatchRange> rr(b->h_ranges.size());
-    BCU(cudaMemcpyAsync(rp.data(), b->d_range_primes, rp.size() * 8, cudaMemcpyDeviceToHost, b->stream));
-    BCU(cudaMemcpyAsync(rr.data(), b->d_ranges, rr.size() * sizeof(BatchRange), cudaMemcpyDeviceToHost, b->stream));
-    BCU(cudaStreamSynchronize(b->stream));
     u64 n = 0;
     bool all = true;
     for (u32 r : J.ranges) {
-        n += rp[r];
-        all = all && rr[r].p_cur >= rr[r].p_end;
+        u64 rp = 0;
+        BatchRange rr;
+        BCU(cudaMemcpyAsync(&rp, b->d_range_primes + r, 8, cudaMemcpyDeviceToHost, b->stream));
+        BCU(cudaMemcpyAsync(&rr, b->d_ranges + r, sizeof rr, cudaMemcpyDeviceToHost, b->stream));
+        BCU(cudaStreamSynchronize(b->stream));
+        n += rp;
+        all = all && rr.p_cur >= rr.p_end;
     }
     if (primes) *primes = n;
     if (done) *done = all ? 1 : 0;

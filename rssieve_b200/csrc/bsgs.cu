@@ -372,16 +372,17 @@ __device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
     }
 }
 
-// Work item i of a batch launch: the group's ranges hold prefix[k+1]-prefix[k]
-// primes each, in record slots range*rcap + (0, 1, ...).
-__device__ __forceinline__ u32 batch_slot(u32 i, const u32 *granges, u32 nr, const u32 *prefix, u32 rcap)
+// Work item i of a batch launch: range slot k contributes prefix[k+1]-prefix[k]
+// primes (0 when it is not in the launch's group), in record slots
+// k*rcap + (0, 1, ...).
+__device__ __forceinline__ u32 batch_slot(u32 i, u32 nr, const u32 *prefix, u32 rcap)
 {
-    u32 lo = 0, hi = nr;                 // last k with prefix[k] <= i
+    u32 lo = 0, hi = nr;                 // last k with prefix[k] <= i (prefix[k+1] > i then)
     while (hi - lo > 1) {
         const u32 mid = (lo + hi) >> 1;
         if (prefix[mid] <= i) lo = mid; else hi = mid;
     }
-    return granges[lo] * rcap + (i - prefix[lo]);
+    return lo * rcap + (i - prefix[lo]);
 }
 
 // MODE: 1 = every prime below 2^63 (Shoup giant steps), 0 = every prime at or
@@ -393,15 +394,14 @@ template <int TPB, int C, int NB, int MODE, bool BATCH>
 __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const PrimeHdr *__restrict__ hdr,
                                                  const u64 *__restrict__ tabs, const u64 *__restrict__ tgt,
                                                  const unsigned char *__restrict__ meta, u32 count, u32 *work_ctr,
-                                                 const BsgsArgs *__restrict__ job_args,
-                                                 const u32 *__restrict__ granges, u32 nr,
+                                                 const BsgsArgs *__restrict__ job_args, u32 nr,
                                                  const u32 *__restrict__ prefix, u32 rcap)
 {
     constexpr u32 NONE = 0xFFFFFFFFu;
     if (BATCH) count = prefix[nr];
     auto slot_of = [&](u32 i) -> u32 {
         if (i >= count) return NONE;
-        return BATCH ? batch_slot(i, granges, nr, prefix, rcap) : i;
+        return BATCH ? batch_slot(i, nr, prefix, rcap) : i;
     };
     constexpr u32 Q = TPB * C;
     static_assert(Q <= 65536, "baby indices are stored in 16 bits");
@@ -594,8 +594,8 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
 template <int G, int MODE, bool BATCH = false>
 static cudaError_t launch_geom(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
                               const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st,
-                              const BsgsArgs *job_args = nullptr, const u32 *granges = nullptr, u32 nr = 0,
-                              const u32 *prefix = nullptr, u32 rcap = 0)
+                              const BsgsArgs *job_args = nullptr, u32 nr = 0, const u32 *prefix = nullptr,
+                              u32 rcap = 0)
 {
     constexpr BsgsGeom g = BSGS_GEOMS[G];
     auto kern = k_bsgs<g.tpb, g.c, g.nb, MODE, BATCH>;
@@ -611,7 +611,7 @@ static cudaError_t launch_geom(const BsgsArgs &a, const PrimeHdr *hdr, const u64
     }
     const u64 want = (u64)sms * (u64)occ;
     const unsigned grid = (unsigned)((BATCH || want < count) ? want : count);
-    kern<<<grid, g.tpb, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr, job_args, granges, nr, prefix, rcap);
+    kern<<<grid, g.tpb, smem, st>>>(a, hdr, tabs, tgt, meta, count, work_ctr, job_args, nr, prefix, rcap);
     return cudaGetLastError();
 }
 
@@ -675,33 +675,37 @@ cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs,
 #undef RS_BSGS_CASE
 }
 
-// prefix[0] = 0, prefix[k+1] = prefix[k] + primes of the group's k-th range (one thread)
-__global__ void k_batch_prefix(const u32 *granges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix)
+// prefix[0] = 0, prefix[k+1] = prefix[k] + primes of range slot k when it is
+// active and in the (geom, shoup) group, else + 0 (one thread; nr is small)
+__global__ void k_batch_prefix(const BatchRange *ranges, u32 nr, int geom, int shoup, const u32 *ctrs, u32 rcap,
+                               u32 *prefix)
 {
     u32 acc = 0;
     prefix[0] = 0;
     for (u32 k = 0; k < nr; ++k) {
-        acc += min(ctrs[granges[k] * BR_CTRS + 1], rcap);
+        const BatchRange R = ranges[k];
+        if (R.active && R.geom == geom && R.shoup == shoup) acc += min(ctrs[k * BR_CTRS + 1], rcap);
         prefix[k + 1] = acc;
     }
 }
 
-cudaError_t launch_batch_prefix(const u32 *group_ranges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix, cudaStream_t st)
+cudaError_t launch_batch_prefix(const BatchRange *ranges, u32 nr, int geom, bool shoup, const u32 *ctrs, u32 rcap,
+                                u32 *prefix, cudaStream_t st)
 {
-    k_batch_prefix<<<1, 1, 0, st>>>(group_ranges, nr, ctrs, rcap, prefix);
+    k_batch_prefix<<<1, 1, 0, st>>>(ranges, nr, geom, shoup ? 1 : 0, ctrs, rcap, prefix);
     return cudaGetLastError();
 }
 
 cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
-                              const u64 *tgt, const unsigned char *meta, const u32 *group_ranges, u32 nr,
-                              const u32 *prefix, u32 rcap, u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st)
+                              const u64 *tgt, const unsigned char *meta, u32 nr, const u32 *prefix, u32 rcap,
+                              u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st)
 {
 #define RS_BSGS_BCASE(G)                                                                                         \
     case G:                                                                                                      \
-        return shoup ? launch_geom<G, 1, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, group_ranges, \
-                                               nr, prefix, rcap)                                                 \
-                     : launch_geom<G, 0, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, group_ranges, \
-                                               nr, prefix, rcap);
+        return shoup ? launch_geom<G, 1, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, nr, prefix, \
+                                               rcap)                                                             \
+                     : launch_geom<G, 0, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, nr, prefix, \
+                                               rcap);
     switch (geom) {
         RS_BSGS_BCASE(0)
         RS_BSGS_BCASE(1)

@@ -50,6 +50,7 @@ extern "C" const char *rs_strerror(int code)
     case RS_ESTATE: return "invalid checkpoint";
     case RS_EVERIFY: return "factor verification failed";
     case RS_ENODEV: return "no CUDA device";
+    case RS_EBUSY: return "no free batch slot";
     default: return "unknown error";
     }
 }

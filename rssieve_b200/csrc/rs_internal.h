@@ -14,6 +14,7 @@ namespace rs {
 
 typedef unsigned long long u64;
 typedef unsigned int u32;
+typedef unsigned char u8;
 
 constexpr int KMAX = 100;            // sequences per job (inputfile.cpp:356-361)
 constexpr int KSTRIDE = 112;         // padded per-prime target stride (16-byte multiple for bulk copies)
@@ -144,9 +145,13 @@ struct BatchWin {
     u64 lo, hi;          // this round's [lo, hi) (lo == hi: the range is done)
     u64 base_odd, nodd;  // odd values base_odd + 2i, i < nodd, covering [lo, hi)
 };
-struct BatchRange {      // device state of one range
+struct BatchRange {      // device state of one range slot
     u64 p_cur, p_end;    // next window start, end of the range
-    u32 job, pad_;
+    u32 job;             // job slot it belongs to
+    u8 active;           // slot in use
+    u8 shoup;            // 1: p_end <= 2^63 (Shoup giant steps), 0: p >= 2^63
+    u8 geom;             // BSGS geometry index of its job
+    u8 pad_;
 };
 // per-range counters of a round: [0] sieve survivors, [1] primes, [2] pad, [3] pad
 constexpr int BR_CTRS = 4;
@@ -180,12 +185,13 @@ cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
                                u32 rcap, const u32 *ctrs, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs, u64 *tgt,
                                unsigned char *meta, u64 *stats, cudaStream_t st);
-// one BSGS launch over the ranges of one (geometry, mode) group: group_ranges
-// lists them, prefix (nr+1 entries) is filled by launch_batch_prefix
-cudaError_t launch_batch_prefix(const u32 *group_ranges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix, cudaStream_t st);
+// one BSGS launch per (geometry, mode) group over range slots [0, nr): prefix
+// (nr+1 entries) counts the primes of the active slots of that group only
+cudaError_t launch_batch_prefix(const BatchRange *ranges, u32 nr, int geom, bool shoup, const u32 *ctrs, u32 rcap,
+                                u32 *prefix, cudaStream_t st);
 cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
-                              const u64 *tgt, const unsigned char *meta, const u32 *group_ranges, u32 nr,
-                              const u32 *prefix, u32 rcap, u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st);
+                              const u64 *tgt, const unsigned char *meta, u32 nr, const u32 *prefix, u32 rcap,
+                              u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st);
 
 }  // namespace rs
 

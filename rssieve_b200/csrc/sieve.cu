@@ -215,7 +215,7 @@ __global__ void k_batch_windows(BatchRange *ranges, BatchWin *wins, u32 nranges,
     BatchWin w;
     w.lo = R.p_cur;
     w.hi = R.p_cur;
-    if (R.p_cur < R.p_end) {
+    if (R.active && R.p_cur < R.p_end) {
         const double lnp = log((double)(R.p_cur < 3 ? 3 : R.p_cur));
         u64 width = (u64)(0.6 * (double)rcap * lnp);
         if (width < 65536) width = 65536;
