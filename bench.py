@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--baby-steps", type=int, default=0, help="fix Q baby steps per prime (0: the per-job tuner)")
+    ap.add_argument("--no-forms", action="store_true", help="skip the batched (config 3) and served (config 5) forms")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     return ap.parse_args()
 
@@ -125,6 +126,75 @@ def cpu_baseline(seed, target_s, job=None):
     return {"value": len(pl) / dt, "unit": "primes/s", "cores": threads, "kind": "port",
             "sample": "%d 2-PRPs from 2^50 (config2 job), %d threads, %.1f s; %.3g Montgomery products/s" % (
                 len(pl), threads, dt, st["mulmods"] / dt)}
+
+
+def measure_batched(torch, rs, W, seed=3, njobs=48, window_log2=24):
+    """Config-3 sample: the same jobs and p-windows through the single-job path, job
+    after job, and through one batch; CUDA events on one side stream bracket each,
+    uploads of the jobs' bitmaps included."""
+    jobs = W.config3(seed, njobs=njobs)
+    seqs = [W.seqs_of(j) for j in jobs]
+    wins = [(j["prange"][0], j["prange"][0] + (1 << window_log2)) for j in jobs]
+    st = torch.cuda.Stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    sv = rs.Sieve(torch.cuda.current_device())
+    sv.set_stream(st.cuda_stream)
+    plain_terms, plain_primes = [], 0
+    torch.cuda.synchronize()
+    ev[0].record(st)
+    for sq, (p0, p1) in zip(seqs, wins):
+        sv.load(sq)
+        plain_primes += sv.run(p0, p1)["primes"]
+        f = sv.factors()
+        plain_terms.append(set(zip(f["seq"].tolist(), f["n"].tolist())))
+    ev[1].record(st)
+    torch.cuda.synchronize()
+    sv.close()
+    b = rs.Batch(torch.cuda.current_device(), max_jobs=njobs, range_slots=njobs + 8)
+    b.set_stream(st.cuda_stream)
+    ev[2].record(st)
+    ids = [b.add(sq, p0, p1) for sq, (p0, p1) in zip(seqs, wins)]
+    b.run(0)
+    ev[3].record(st)
+    torch.cuda.synchronize()
+    batch_primes = sum(b.job_info(j)[1] for j in ids)
+    same = all(set(zip(f["seq"].tolist(), f["n"].tolist())) == t
+               for f, t in zip((b.factors(j) for j in ids), plain_terms))
+    qs = sorted(set(b.job_info(j)[0] for j in ids))
+    b.close()
+    pms, bms = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
+    return {"workload": "config3 sample: %d jobs (1-100 seqs, b in {2,3,5,6,10}, n from 1e6, p from 2^44..2^60), "
+                        "2^%d-wide p-window each" % (njobs, window_log2),
+            "primes": int(batch_primes), "plain_primes_per_s": plain_primes / (pms / 1e3),
+            "batched_primes_per_s": batch_primes / (bms / 1e3), "batched_over_plain": pms / bms,
+            "identical_eliminated_terms": bool(same and plain_primes == batch_primes), "baby_steps_used": qs}
+
+
+def measure_served(rs, W, serve, seed=5, nunits=60, rate=8.0, width_log2=(22, 26)):
+    """Config-5 shape, scaled down: 16 config-2-style files, Poisson arrivals at `rate`
+    units/s, unit widths 2^22..2^26 (the full workload's are 2^30..2^36); latency
+    from arrival and from admission, and each unit's latency over its own run time
+    alone on the same server."""
+    import numpy as np
+    files = [W.seqs_of(f) for f in W.config5_files(seed)]
+    raw = W.config5_units(seed, nunits, rate, len(files), width_log2)
+    units = [serve.Unit(k, fi, p0, p1, t) for k, (t, fi, p0, p1) in enumerate(raw)]
+    srv = serve.Server(files, max_units=48, range_slots=64)
+    try:
+        out = srv.run(units)
+        st = serve.latency_stats(out)
+        ratios = []
+        for u in out:
+            v = serve.Unit(u.uid, u.file, u.p0, u.p1, 0.0)
+            srv.run([v])
+            ratios.append((u.finished - u.arrival) / max(v.finished - v.admitted, 1e-6))
+    finally:
+        srv.close()
+    st.update({"workload": "config5 shape scaled down: %d units over 16 files, Poisson %.0f units/s, widths 2^%d..2^%d, "
+                           "starts 2^44..2^62" % (nunits, rate, width_log2[0], width_log2[1]),
+               "latency_over_isolated_p50": float(np.percentile(ratios, 50)),
+               "latency_over_isolated_p99": float(np.percentile(ratios, 99))})
+    return st
 
 
 def run_reference(args):
@@ -270,6 +340,11 @@ def main():
     if rank == 0 and world == 1:
         cpu = cpu_baseline(args.seed, args.cpu_seconds, job)
 
+    forms = None
+    if rank == 0 and world == 1 and not args.no_forms:
+        from rssieve_b200 import serve
+        forms = {"batched": measure_batched(torch, rs, W), "served": measure_served(rs, W, serve)}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "primes/s", "n_gpus": world, "steps": args.steps,
@@ -287,6 +362,7 @@ def main():
                          "traffic_unit": "bytes per BSGS launch (ncu per-prime DRAM bytes x primes per launch)",
                          "peak_source": "measured live: rs_mulmod_peak, independent Montgomery-product chains"},
             "cpu_baseline": cpu,
+            "forms": forms,
             "clocks": clocks,
             "detail": {"primes": tot["primes"], "giant_steps": tot["giant"], "baby_steps": tot["baby"],
                        "targets_per_prime": tot["targets"] / max(tot["full"] + tot["parity"], 1),

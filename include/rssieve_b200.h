@@ -203,11 +203,15 @@ int rs_batch_set_stream(rs_batch *b, void *stream);
  * RS_EBUSY when no job or range slot is free. */
 int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t p1, uint32_t q, uint32_t *job);
 /* A new job with job src's sequences, geometry and current bitmap, copied on
- * the device (no host transfer), over [p0, p1).  A job added with p0 == p1 is
- * a resident template: it takes no range slot and never runs, and serves as
- * the source of clones -- e.g. one template per input file, one clone per
- * work unit, each unit with its own bitmap. */
-int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64_t p1, uint32_t *job);
+ * the device (no host transfer), over [p0, p1) cut into nsplit equal parts
+ * (one range slot each, sharing the bitmap), so that a unit can spread over
+ * the device.  A job added with p0 == p1 is a resident template: it takes no
+ * range slot and never runs, and serves as the source of clones -- e.g. one
+ * template per input file, one clone per work unit, each unit with its own
+ * bitmap. */
+int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64_t p1, uint32_t nsplit, uint32_t *job);
+/* Free job slots and range slots. */
+int rs_batch_free_slots(rs_batch *b, uint32_t *jobs, uint32_t *ranges);
 /* Frees a job's slots (fetch its factors and bitmap first). */
 int rs_batch_release(rs_batch *b, uint32_t job);
 /* Runs up to max_rounds rounds (0: until every job is done); *done = 1 once

@@ -52,7 +52,7 @@ EXPORTS = (
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
     "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_primes_generate_noalloc",
     "rs_set_baby_steps", "rs_get_baby_steps",
-    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone", "rs_batch_release", "rs_batch_run",
+    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone", "rs_batch_free_slots", "rs_batch_release", "rs_batch_run",
     "rs_batch_factors_fetch", "rs_batch_bitmap_download", "rs_batch_job_info", "rs_batch_counters",
 )
 BABY_STEPS = (1024, 2048, 4096, 8192, 16384)   # accepted by rs_set_baby_steps (0: automatic)
@@ -107,7 +107,8 @@ def lib():
         "rs_set_baby_steps": (C.c_int, [vp, u32]),
         "rs_batch_create": (C.c_int, [C.c_int, u32, u32, C.POINTER(vp)]),
         "rs_batch_release": (C.c_int, [vp, u32]),
-        "rs_batch_add_clone": (C.c_int, [vp, u32, u64, u64, C.POINTER(u32)]),
+        "rs_batch_add_clone": (C.c_int, [vp, u32, u64, u64, u32, C.POINTER(u32)]),
+        "rs_batch_free_slots": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
         "rs_batch_destroy": (None, [vp]),
         "rs_batch_set_stream": (C.c_int, [vp, vp]),
         "rs_batch_add": (C.c_int, [vp, PS, u64, u64, u32, C.POINTER(u32)]),
@@ -373,6 +374,10 @@ class Batch:
         except Exception:
             pass
 
+    def set_stream(self, stream_handle):
+        """Run the batch's rounds on a caller stream (not the legacy default stream)."""
+        _check(lib().rs_batch_set_stream(self._b, C.c_void_p(stream_handle)), "rs_batch_set_stream")
+
     def add(self, seqs, p0, p1, q=0):
         """Add a job over [p0, p1); returns its slot, or None when no slot is free."""
         j = C.c_uint32(0)
@@ -383,15 +388,22 @@ class Batch:
         self._seqs[j.value] = seqs
         return j.value
 
-    def add_clone(self, src, p0, p1):
-        """A job copying slot src's sequences and bitmap on the device; None when no slot is free."""
+    def add_clone(self, src, p0, p1, nsplit=1):
+        """A job copying slot src's sequences and bitmap on the device, its p-range cut into
+        nsplit range slots; None when no slot is free."""
         j = C.c_uint32(0)
-        rc = lib().rs_batch_add_clone(self._b, src, p0, p1, C.byref(j))
+        rc = lib().rs_batch_add_clone(self._b, src, p0, p1, nsplit, C.byref(j))
         if rc in (RS_EBUSY, RS_ENOMEM):
             return None
         _check(rc, "rs_batch_add_clone")
         self._seqs[j.value] = self._seqs[src]
         return j.value
+
+    def free_slots(self):
+        """(free job slots, free range slots)."""
+        j, r = C.c_uint32(0), C.c_uint32(0)
+        _check(lib().rs_batch_free_slots(self._b, C.byref(j), C.byref(r)), "rs_batch_free_slots")
+        return j.value, r.value
 
     def release(self, job):
         _check(lib().rs_batch_release(self._b, job), "rs_batch_release")

@@ -242,7 +242,7 @@ extern "C" int rs_batch_set_stream(rs_batch *b, void *stream)
 }
 
 static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_t p0, uint64_t p1, uint32_t q,
-                         uint32_t *job);
+                         uint32_t nsplit, uint32_t *job);
 
 extern "C" int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t p1, uint32_t q, uint32_t *job)
 {
@@ -257,13 +257,14 @@ extern "C" int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t
         rs_set_error("rs_batch_add: p1 < p0");
         return RS_EARG;
     }
-    return batch_add_job(b, s, nullptr, p0, p1, q, job);
+    return batch_add_job(b, s, nullptr, p0, p1, q, 1, job);
 }
 
 // Adds a job from host sequences s, or (s == nullptr) as a copy of job slot src
 // made on the device.  p0 == p1: a resident template that takes no range slot.
+// The p-range is cut into nsplit equal parts, and at 2^63, one range slot each.
 static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_t p0, uint64_t p1, uint32_t q,
-                         uint32_t *job)
+                         uint32_t nsplit, uint32_t *job)
 {
     const bool tmpl = (p0 == p1);
     if (p0 < 3) p0 = 3;
@@ -272,7 +273,19 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
         return RS_EARG;
     }
     const u64 TOP = 1ull << 63;
-    const u32 need = tmpl ? 0 : (p0 < TOP && p1 > TOP) ? 2 : 1;
+    std::vector<u64> cuts;                   // range boundaries p0 = c0 < c1 < ... < p1
+    if (!tmpl) {
+        if (nsplit < 1) nsplit = 1;
+        if (nsplit > p1 - p0) nsplit = (u32)(p1 - p0);
+        const u64 w = (p1 - p0) / nsplit;
+        cuts.push_back(p0);
+        for (u32 i = 1; i < nsplit; ++i) cuts.push_back(p0 + i * w);
+        if (p0 < TOP && p1 > TOP) cuts.push_back(TOP);
+        cuts.push_back(p1);
+        std::sort(cuts.begin(), cuts.end());
+        cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
+    }
+    const u32 need = tmpl ? 0 : (u32)cuts.size() - 1;
     u32 jid = 0;
     while (jid < b->max_jobs && b->jobs[jid].used) ++jid;
     std::vector<u32> slots;
@@ -331,10 +344,9 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
     BCU(cudaMemcpyAsync(b->d_geoms + jid, &G, sizeof G, cudaMemcpyHostToDevice, b->stream));
     BCU(cudaMemcpyAsync(b->d_args + jid, &A, sizeof A, cudaMemcpyHostToDevice, b->stream));
     BCU(cudaMemsetAsync(b->d_fctrs + jid, 0, 4, b->stream));
-    u64 lo = p0;
     for (u32 i = 0; i < need; ++i) {
         const u32 r = slots[i];
-        const u64 hi = (need == 2 && i == 0) ? TOP : p1;
+        const u64 lo = cuts[i], hi = cuts[i + 1];
         BatchRange R;
         memset(&R, 0, sizeof R);
         R.p_cur = lo;
@@ -348,11 +360,21 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
         J.ranges.push_back(r);
         BCU(cudaMemcpyAsync(b->d_ranges + r, &b->h_ranges[r], sizeof R, cudaMemcpyHostToDevice, b->stream));
         BCU(cudaMemsetAsync(b->d_range_primes + r, 0, 8, b->stream));
-        lo = hi;
     }
     BCU(cudaStreamSynchronize(b->stream));     // the host structs above go out of scope
     b->done = false;
     if (job) *job = jid;
+    return RS_OK;
+}
+
+extern "C" int rs_batch_free_slots(rs_batch *b, uint32_t *jobs, uint32_t *ranges)
+{
+    if (!b) return RS_EARG;
+    u32 fj = 0, fr = 0;
+    for (const auto &j : b->jobs) fj += j.used ? 0 : 1;
+    for (char u : b->range_used) fr += u ? 0 : 1;
+    if (jobs) *jobs = fj;
+    if (ranges) *ranges = fr;
     return RS_OK;
 }
 
@@ -375,7 +397,7 @@ extern "C" int rs_batch_release(rs_batch *b, uint32_t job)
     return RS_OK;
 }
 
-extern "C" int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64_t p1, uint32_t *job)
+extern "C" int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64_t p1, uint32_t nsplit, uint32_t *job)
 {
     if (!b || src >= b->max_jobs || !b->jobs[src].used) return RS_EARG;
     if (p1 <= p0 || p1 <= 3) {
@@ -383,7 +405,7 @@ extern "C" int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64
         return RS_EARG;
     }
     const BJob copy = b->jobs[src];          // the slot vector is not resized, but keep a stable copy
-    return batch_add_job(b, nullptr, &copy, p0, p1, 0, job);
+    return batch_add_job(b, nullptr, &copy, p0, p1, 0, nsplit, job);
 }
 
 // Enqueues one round on b->stream (also what the graph captures).

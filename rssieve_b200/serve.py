@@ -6,11 +6,13 @@ batch template (rs_batch_add with an empty range); a unit is admitted as a
 device-side clone of its file's template with its own bitmap, so its result
 does not depend on which other units share the device.  Admission is by free
 batch slots and device memory: a unit that arrives while others are running
-joins at the next round boundary, runs alongside them (one BSGS launch per
+joins at the next round boundary, spread over as many free range slots as
+finish it in about one round, runs alongside them (one BSGS launch per
 geometry group covers every admitted unit), and leaves when its range is done
 -- its factors and bitmap are collected and its slots released for the next
 arrival.  Latency is measured from arrival and from admission.
 """
+import math
 import time
 from dataclasses import dataclass, field
 
@@ -36,10 +38,13 @@ class Unit:
 class Server:
     """Continuous-batching sieve server over one device."""
 
-    def __init__(self, files, device=0, max_units=48, range_slots=None):
-        # template slots + unit slots; a unit takes one range slot (two if it straddles 2^63)
+    # primes one range slot covers per round (0.6 of the batch's 65536-prime round capacity)
+    PRIMES_PER_SLOT_ROUND = 0.6 * 65536
+
+    def __init__(self, files, device=0, max_units=48, range_slots=64):
+        # template slots + unit slots; a unit spreads over one or more range slots
         nf = len(files)
-        self.batch = Batch(device, max_jobs=nf + max_units, range_slots=range_slots or max_units)
+        self.batch = Batch(device, max_jobs=nf + max_units, range_slots=range_slots)
         self.templates = []
         for seqs in files:
             t = self.batch.add(seqs, 3, 3)        # p0 == p1: resident template, never runs
@@ -61,10 +66,16 @@ class Server:
             while i < len(pending) and pending[i].arrival <= now:
                 queue.append(pending[i])
                 i += 1
-            # admit in arrival order while slots and memory allow
+            # admit in arrival order while slots and memory allow; a unit takes as many
+            # free range slots as finish it in about one round
             while queue and len(active) < self.max_units:
                 u = queue[0]
-                slot = self.batch.add_clone(self.templates[u.file], u.p0, u.p1)
+                free = self.batch.free_slots()[1]
+                if free == 0:
+                    break
+                est = (u.p1 - u.p0) / math.log(max(u.p0, 3))
+                nsplit = max(1, min(free, math.ceil(est / self.PRIMES_PER_SLOT_ROUND)))
+                slot = self.batch.add_clone(self.templates[u.file], u.p0, u.p1, nsplit)
                 if slot is None:
                     break
                 u.admitted = clock() - t0

@@ -139,13 +139,14 @@ def config5_files(seed=5, nfiles=16):
     return files
 
 
-def config5_units(seed=5, nunits=10000, rate=100.0, nfiles=16):
-    """Poisson arrivals: list of (arrival_s, file_index, p0, p1)."""
+def config5_units(seed=5, nunits=10000, rate=100.0, nfiles=16, width_log2=(30, 36)):
+    """Poisson arrivals: list of (arrival_s, file_index, p0, p1); widths 2^U{width_log2}
+    (30..36 for the full workload; a scaled-down run passes smaller exponents)."""
     g = SplitMix64(seed + 77)
     t, units = 0.0, []
     for _ in range(nunits):
         t += -math.log(1.0 - g.real()) / rate
-        w = 1 << g.uniform(30, 37)
+        w = 1 << g.uniform(width_log2[0], width_log2[1] + 1)
         p0 = g.log_uniform(1 << 44, 1 << 62)
         units.append((t, g.uniform(0, nfiles), p0, p0 + w))
     return units

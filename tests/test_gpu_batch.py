@@ -103,3 +103,30 @@ def test_batch_config3_shapes_match_single_job_path(rs, sieve):
             assert b.job_info(j)[1] == cnt["primes"]
     finally:
         b.close()
+
+
+def test_clone_split_over_range_slots_matches_single_job_path(rs, sieve):
+    """A template job cloned over a p-range cut into 7 range slots (one bitmap
+    shared by the 7 ranges) gives the single-job path's result."""
+    job = W.small_job(58, kcount=16, base=2, nmin=20000, nmax=120000, keep=0.2, kmax=1 << 26)
+    seqs = W.seqs_of(job)
+    p0, p1 = 2_000_000, 2_600_000
+    b = rs.Batch(0, max_jobs=4, range_slots=8)
+    try:
+        t = b.add(seqs, 3, 3)                       # resident template
+        assert b.job_info(t)[1:] == (0, True)
+        j = b.add_clone(t, p0, p1, nsplit=7)
+        assert b.free_slots() == (2, 1)
+        assert b.run(0)
+        sieve.load(seqs)
+        cnt = sieve.run(p0, p1)
+        f = sieve.factors()
+        assert len(f) > 0
+        assert _terms(b.factors(j)) == _terms(f)
+        assert np.array_equal(b.bitmap(j), sieve.bitmap())
+        assert b.job_info(j)[1] == cnt["primes"]
+        assert np.array_equal(b.bitmap(t), seqs.bitmap)         # the template is untouched
+        b.release(j)
+        assert b.free_slots() == (3, 8)
+    finally:
+        b.close()
