@@ -210,12 +210,22 @@ int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t p1, uint32
  * template per input file, one clone per work unit, each unit with its own
  * bitmap. */
 int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64_t p1, uint32_t nsplit, uint32_t *job);
+/* Primes a job should cover in each following round, spread over its
+ * unfinished ranges (each range at most about 39 000 per round); 0 pauses it.
+ * Jobs start with full windows.  A serving loop sets these per round to order
+ * work (e.g. shortest remaining first). */
+int rs_batch_set_budget(rs_batch *b, uint32_t job, uint64_t primes);
+/* Every job slot's state in one read: done (job finished; 0 for free slots),
+ * primes tested and p-range left to sieve -- arrays of max_jobs entries, each
+ * may be NULL. */
+int rs_batch_poll(rs_batch *b, uint8_t *done, uint64_t *primes, uint64_t *remaining);
 /* Free job slots and range slots. */
 int rs_batch_free_slots(rs_batch *b, uint32_t *jobs, uint32_t *ranges);
 /* Frees a job's slots (fetch its factors and bitmap first). */
 int rs_batch_release(rs_batch *b, uint32_t job);
-/* Runs up to max_rounds rounds (0: until every job is done); *done = 1 once
- * every job's p-range is finished. */
+/* Runs up to max_rounds rounds (0: until every job is done, or every
+ * unfinished job is paused by a zero budget); *done = 1 once every job's
+ * p-range is finished. */
 int rs_batch_run(rs_batch *b, uint32_t max_rounds, int *done);
 /* Per job, as rs_factors_fetch / rs_bitmap_download. */
 int rs_batch_factors_fetch(rs_batch *b, uint32_t job, rs_factor *buf, size_t cap, size_t *n);

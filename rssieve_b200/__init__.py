@@ -52,7 +52,8 @@ EXPORTS = (
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
     "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_primes_generate_noalloc",
     "rs_set_baby_steps", "rs_get_baby_steps",
-    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone", "rs_batch_free_slots", "rs_batch_release", "rs_batch_run",
+    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone", "rs_batch_free_slots", "rs_batch_release", "rs_batch_set_budget",
+    "rs_batch_poll", "rs_batch_run",
     "rs_batch_factors_fetch", "rs_batch_bitmap_download", "rs_batch_job_info", "rs_batch_counters",
 )
 BABY_STEPS = (1024, 2048, 4096, 8192, 16384)   # accepted by rs_set_baby_steps (0: automatic)
@@ -109,6 +110,8 @@ def lib():
         "rs_batch_release": (C.c_int, [vp, u32]),
         "rs_batch_add_clone": (C.c_int, [vp, u32, u64, u64, u32, C.POINTER(u32)]),
         "rs_batch_free_slots": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
+        "rs_batch_set_budget": (C.c_int, [vp, u32, u64]),
+        "rs_batch_poll": (C.c_int, [vp, vp, vp, vp]),
         "rs_batch_destroy": (None, [vp]),
         "rs_batch_set_stream": (C.c_int, [vp, vp]),
         "rs_batch_add": (C.c_int, [vp, PS, u64, u64, u32, C.POINTER(u32)]),
@@ -362,6 +365,7 @@ class Batch:
         self._b = C.c_void_p()
         _check(L.rs_batch_create(device, max_jobs, range_slots, C.byref(self._b)), "rs_batch_create")
         self._seqs = {}
+        self.max_jobs = max_jobs or 64
 
     def close(self):
         if getattr(self, "_b", None) and self._b.value:
@@ -404,6 +408,18 @@ class Batch:
         j, r = C.c_uint32(0), C.c_uint32(0)
         _check(lib().rs_batch_free_slots(self._b, C.byref(j), C.byref(r)), "rs_batch_free_slots")
         return j.value, r.value
+
+    def set_budget(self, job, primes):
+        """Primes the job should cover per round from now on (0 pauses it)."""
+        _check(lib().rs_batch_set_budget(self._b, job, int(primes)), "rs_batch_set_budget")
+
+    def poll(self):
+        """(done, primes tested, p-range left) for every job slot, from one device read."""
+        d = np.zeros(self.max_jobs, dtype=np.uint8)
+        n = np.zeros(self.max_jobs, dtype=np.uint64)
+        r = np.zeros(self.max_jobs, dtype=np.uint64)
+        _check(lib().rs_batch_poll(self._b, d.ctypes.data, n.ctypes.data, r.ctypes.data), "rs_batch_poll")
+        return d.astype(bool), n, r
 
     def release(self, job):
         _check(lib().rs_batch_release(self._b, job), "rs_batch_release")

@@ -90,6 +90,11 @@ struct rs_batch {
     std::vector<BJob> jobs;
     std::vector<BatchRange> h_ranges;      // host copy of the range slots' fixed fields
     std::vector<char> range_used;
+    std::vector<u32> h_win;                // primes per round per range slot (0: paused)
+    std::vector<char> range_done;          // from the last rs_batch_poll
+    bool win_dirty = false;
+    u32 *d_win = nullptr;
+    u32 *h_win_pin = nullptr;
     std::vector<Group> groups;
     // device tables
     u32 *d_sp = nullptr;
@@ -145,9 +150,10 @@ extern "C" void rs_batch_destroy(rs_batch *b)
     }
     void *ptrs[] = {b->d_sp, b->d_jobs, b->d_geoms, b->d_args, b->d_fctrs, b->d_ranges, b->d_wins, b->d_ctrs,
                     b->d_range_primes, b->d_cands, b->d_primes, b->d_hdr, b->d_aux, b->d_tabs, b->d_tgt, b->d_meta,
-                    b->d_err, b->d_stats, b->d_unfinished};
+                    b->d_err, b->d_stats, b->d_unfinished, b->d_win};
     for (void *p : ptrs) cudaFree(p);
     if (b->h_pin) cudaFreeHost(b->h_pin);
+    if (b->h_win_pin) cudaFreeHost(b->h_win_pin);
     if (b->own) cudaStreamDestroy(b->own);
     delete b;
 }
@@ -183,6 +189,8 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
     b->jobs.resize(max_jobs);
     b->h_ranges.assign(range_slots, BatchRange{});
     b->range_used.assign(range_slots, 0);
+    b->h_win.assign(range_slots, 0);
+    b->range_done.assign(range_slots, 0);
     const u32 J = max_jobs, R = range_slots;
     std::vector<u32> sp = rs_small_primes();
     b->nsp = (u32)sp.size();
@@ -198,7 +206,8 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         !alloc(&b->d_aux, (size_t)R * RCAP * setup_aux_bytes()) ||
         !alloc((void **)&b->d_tabs, (size_t)R * RCAP * TABS * 8) ||
         !alloc((void **)&b->d_tgt, (size_t)R * RCAP * KSTRIDE * 8) ||
-        !alloc((void **)&b->d_meta, (size_t)R * RCAP * KSTRIDE) || cudaMallocHost(&b->h_pin, 16) != cudaSuccess) {
+        !alloc((void **)&b->d_meta, (size_t)R * RCAP * KSTRIDE) || !alloc((void **)&b->d_win, R * 4) ||
+        cudaMallocHost(&b->h_pin, 16) != cudaSuccess || cudaMallocHost(&b->h_win_pin, R * 4) != cudaSuccess) {
         rs_set_error("cannot allocate a batch of %u range slots (about %zu MB)", R,
                      (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 9 + 24 + 8 + 16) >> 20);
         return fail(RS_ENOMEM);
@@ -210,7 +219,7 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         cudaMemset(b->d_args, 0, J * sizeof(BsgsArgs)) != cudaSuccess || cudaMemset(b->d_fctrs, 0, J * 4) != cudaSuccess ||
         cudaMemset(b->d_ranges, 0, R * sizeof(BatchRange)) != cudaSuccess ||
         cudaMemset(b->d_ctrs, 0, (size_t)R * BR_CTRS * 4) != cudaSuccess ||
-        cudaMemset(b->d_range_primes, 0, R * 8) != cudaSuccess)
+        cudaMemset(b->d_range_primes, 0, R * 8) != cudaSuccess || cudaMemset(b->d_win, 0, R * 4) != cudaSuccess)
         return fail(RS_ECUDA);
     if (bsgs_prepare() != cudaSuccess) {
         rs_set_error("cannot configure the BSGS kernels' shared memory");
@@ -357,6 +366,9 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
         R.geom = (u8)J.geom;
         b->h_ranges[r] = R;
         b->range_used[r] = 1;
+        b->range_done[r] = 0;
+        b->h_win[r] = (u32)(0.6 * RCAP);       // full windows until a budget is set
+        b->win_dirty = true;
         J.ranges.push_back(r);
         BCU(cudaMemcpyAsync(b->d_ranges + r, &b->h_ranges[r], sizeof R, cudaMemcpyHostToDevice, b->stream));
         BCU(cudaMemsetAsync(b->d_range_primes + r, 0, 8, b->stream));
@@ -388,6 +400,8 @@ extern "C" int rs_batch_release(rs_batch *b, uint32_t job)
         memset(&R, 0, sizeof R);
         b->h_ranges[r] = R;
         b->range_used[r] = 0;
+        b->h_win[r] = 0;
+        b->win_dirty = true;
         BCU(cudaMemcpyAsync(b->d_ranges + r, &b->h_ranges[r], sizeof R, cudaMemcpyHostToDevice, b->stream));
     }
     BCU(cudaFreeAsync(J.d_bitmap, b->stream));
@@ -416,7 +430,7 @@ static int batch_round(rs_batch *b)
     // widest window: 0.6*RCAP*ln(2^64) values, i.e. 0.3*RCAP*44.4 odd values
     const u32 max_blocks = (u32)((0.3 * RCAP * 44.4) / (SIEVE_WORDS * 32.0)) + 2;
     BCU(cudaMemsetAsync(b->d_unfinished, 0, 4, st));
-    BCU(launch_batch_windows(b->d_ranges, b->d_wins, R, RCAP, b->d_ctrs, st));
+    BCU(launch_batch_windows(b->d_ranges, b->d_wins, b->d_win, R, RCAP, b->d_ctrs, st));
     BCU(launch_sieve_batch(b->d_wins, R, max_blocks, b->d_sp, b->nsp, b->d_cands, CCAP, b->d_ctrs, b->d_err, st));
     BCU(launch_mr_batch(b->d_cands, CCAP, b->d_primes, RCAP, b->d_ctrs, R, b->d_err, b->sms, st));
     BCU(launch_setup_batch(b->d_jobs, b->d_geoms, b->d_ranges, b->d_primes, RCAP, b->d_ctrs, R, b->d_hdr, b->d_aux,
@@ -445,6 +459,11 @@ extern "C" int rs_batch_run(rs_batch *b, uint32_t max_rounds, int *done)
     for (char u : b->range_used) any = any || u;
     if (!any) b->done = true;
     for (uint32_t i = 0; (max_rounds == 0 || i < max_rounds) && !b->done; ++i) {
+        if (b->win_dirty) {                          // per-slot round targets, read by the round's first kernel
+            memcpy(b->h_win_pin, b->h_win.data(), b->nranges * 4);
+            BCU(cudaMemcpyAsync(b->d_win, b->h_win_pin, b->nranges * 4, cudaMemcpyHostToDevice, b->stream));
+            b->win_dirty = false;
+        }
         if (b->rounds == 0) {
             int rc = batch_round(b);                 // eager: sizes the persistent grids
             if (rc) return rc;
@@ -473,8 +492,58 @@ extern "C" int rs_batch_run(rs_batch *b, uint32_t max_rounds, int *done)
             return RS_EDEVICE;
         }
         b->done = (b->h_pin[1] == 0);
+        bool any_win = false;
+        for (u32 r = 0; r < b->nranges; ++r) any_win = any_win || (b->range_used[r] && b->h_win[r]);
+        if (!any_win) break;                         // every unfinished range is paused: nothing to run
     }
     if (done) *done = b->done ? 1 : 0;
+    return RS_OK;
+}
+
+extern "C" int rs_batch_set_budget(rs_batch *b, uint32_t job, uint64_t primes)
+{
+    if (!b || job >= b->max_jobs || !b->jobs[job].used) return RS_EARG;
+    const BJob &J = b->jobs[job];
+    u32 live = 0;
+    for (u32 r : J.ranges) live += b->range_done[r] ? 0 : 1;
+    const u64 cap = (u64)(0.6 * RCAP);
+    for (u32 r : J.ranges) {
+        u64 w = 0;
+        if (!b->range_done[r] && live) w = (primes + live - 1) / live;
+        if (w > cap) w = cap;
+        if (b->h_win[r] != (u32)w) {
+            b->h_win[r] = (u32)w;
+            b->win_dirty = true;
+        }
+    }
+    return RS_OK;
+}
+
+extern "C" int rs_batch_poll(rs_batch *b, uint8_t *done, uint64_t *primes, uint64_t *remaining)
+{
+    if (!b) return RS_EARG;
+    BCU(cudaSetDevice(b->device));
+    const u32 R = b->nranges;
+    std::vector<BatchRange> rr(R);
+    std::vector<u64> rp(R);
+    BCU(cudaMemcpyAsync(rr.data(), b->d_ranges, R * sizeof(BatchRange), cudaMemcpyDeviceToHost, b->stream));
+    BCU(cudaMemcpyAsync(rp.data(), b->d_range_primes, R * 8, cudaMemcpyDeviceToHost, b->stream));
+    BCU(cudaStreamSynchronize(b->stream));
+    for (u32 j = 0; j < b->max_jobs; ++j) {
+        const BJob &J = b->jobs[j];
+        u64 n = 0, rem = 0;
+        bool all = true;
+        for (u32 r : J.ranges) {
+            const bool fin = rr[r].p_cur >= rr[r].p_end;
+            b->range_done[r] = fin ? 1 : 0;
+            n += rp[r];
+            rem += fin ? 0 : rr[r].p_end - rr[r].p_cur;
+            all = all && fin;
+        }
+        if (done) done[j] = (J.used && all) ? 1 : 0;
+        if (primes) primes[j] = n;
+        if (remaining) remaining[j] = rem;
+    }
     return RS_OK;
 }
 

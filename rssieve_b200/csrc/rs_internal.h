@@ -177,7 +177,9 @@ cudaError_t bsgs_prepare();   // per device, before the first launch
 cudaError_t launch_mulmod_peak(u64 *out, int blocks, int iters, cudaStream_t st);
 
 // batch rounds (sieve.cu, setup.cu, bsgs.cu)
-cudaError_t launch_batch_windows(BatchRange *ranges, BatchWin *wins, u32 nranges, u32 rcap, u32 *ctrs, cudaStream_t st);
+// win[r]: primes range slot r should cover this round (0: none); capped at 0.6*rcap
+cudaError_t launch_batch_windows(BatchRange *ranges, BatchWin *wins, const u32 *win, u32 nranges, u32 rcap, u32 *ctrs,
+                                 cudaStream_t st);
 cudaError_t launch_sieve_batch(const BatchWin *wins, u32 nranges, u32 max_blocks, const u32 *sp, u32 nsp, u64 *cands,
                                u32 ccap, u32 *ctrs, u32 *err, cudaStream_t st);
 cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges, u32 *err,

@@ -204,10 +204,11 @@ __global__ void __launch_bounds__(256) k_mr_batch(const u64 *__restrict__ cands,
             ctrs + r * BR_CTRS + 1, err);
 }
 
-// Next window of every range, sized for about 0.6*rcap primes (width
-// 0.6*rcap*ln p) and clamped to the range's end (a range lies entirely on one
-// side of 2^63).  Also clears the range's counters.
-__global__ void k_batch_windows(BatchRange *ranges, BatchWin *wins, u32 nranges, u32 rcap, u32 *ctrs)
+// Next window of every range, sized for win[r] primes (width win*ln p, at
+// most 0.6*rcap primes: the slot's capacity with a wide margin) and clamped to
+// the range's end (a range lies entirely on one side of 2^63).  Also clears
+// the range's counters.
+__global__ void k_batch_windows(BatchRange *ranges, BatchWin *wins, const u32 *win, u32 nranges, u32 rcap, u32 *ctrs)
 {
     const u32 r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nranges) return;
@@ -215,10 +216,11 @@ __global__ void k_batch_windows(BatchRange *ranges, BatchWin *wins, u32 nranges,
     BatchWin w;
     w.lo = R.p_cur;
     w.hi = R.p_cur;
-    if (R.active && R.p_cur < R.p_end) {
+    const double target = min((double)win[r], 0.6 * (double)rcap);
+    if (R.active && R.p_cur < R.p_end && target > 0) {
         const double lnp = log((double)(R.p_cur < 3 ? 3 : R.p_cur));
-        u64 width = (u64)(0.6 * (double)rcap * lnp);
-        if (width < 65536) width = 65536;
+        u64 width = (u64)(target * lnp);
+        if (width < 4096) width = 4096;
         w.hi = (R.p_end - R.p_cur > width) ? R.p_cur + width : R.p_end;
     }
     u64 lo = w.lo < 3 ? 3 : w.lo;
@@ -240,9 +242,10 @@ cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp,
     return cudaGetLastError();
 }
 
-cudaError_t launch_batch_windows(BatchRange *ranges, BatchWin *wins, u32 nranges, u32 rcap, u32 *ctrs, cudaStream_t st)
+cudaError_t launch_batch_windows(BatchRange *ranges, BatchWin *wins, const u32 *win, u32 nranges, u32 rcap, u32 *ctrs,
+                                 cudaStream_t st)
 {
-    k_batch_windows<<<(nranges + 127) / 128, 128, 0, st>>>(ranges, wins, nranges, rcap, ctrs);
+    k_batch_windows<<<(nranges + 127) / 128, 128, 0, st>>>(ranges, wins, win, nranges, rcap, ctrs);
     return cudaGetLastError();
 }
 

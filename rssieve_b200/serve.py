@@ -6,11 +6,12 @@ batch template (rs_batch_add with an empty range); a unit is admitted as a
 device-side clone of its file's template with its own bitmap, so its result
 does not depend on which other units share the device.  Admission is by free
 batch slots and device memory: a unit that arrives while others are running
-joins at the next round boundary, spread over as many free range slots as
-finish it in about one round, runs alongside them (one BSGS launch per
+joins at the next round boundary, spread over a few free range slots, runs
+alongside them (one BSGS launch per
 geometry group covers every admitted unit), and leaves when its range is done
 -- its factors and bitmap are collected and its slots released for the next
-arrival.  Latency is measured from arrival and from admission.
+arrival.  Every round the units share a budget of work, shortest remaining
+first.  Latency is measured from arrival and from admission.
 """
 import math
 import time
@@ -35,30 +36,67 @@ class Unit:
     bitmap: np.ndarray = field(default=None, repr=False)
 
 
-class Server:
-    """Continuous-batching sieve server over one device."""
+def cost_per_prime(q, kcount, L):
+    """Model cost of one prime in baby-step units for Q baby steps (the library's
+    geometry model: Q baby steps plus the giant steps of the surviving targets)."""
+    m = -(-L // q)
+    return 1.15 * q + 1.2 * 0.6 * kcount * 0.75 * m
 
-    # primes one range slot covers per round (0.6 of the batch's 65536-prime round capacity)
-    PRIMES_PER_SLOT_ROUND = 0.6 * 65536
+
+class Server:
+    """Continuous-batching sieve server over one device.
+
+    Each round, units are ordered by their estimated remaining work (primes
+    left times the model cost of one prime for their file) and given primes to
+    cover from a round budget -- shortest remaining first -- so that a short
+    unit arriving while long ones run finishes within a round or two.  The
+    budget is ROUND_S seconds of the measured throughput.  A unit spreads over
+    at most MAX_SPLIT range slots, enough to take a whole round's budget, so
+    that slots stay free for arrivals."""
+
+    PRIMES_PER_SLOT_ROUND = 0.6 * 65536    # one range slot's round capacity
+    ROUND_S = 0.006                        # target round duration
+    MAX_SPLIT = 8                          # range slots per unit: a few absorb a round's budget,
+                                           # the rest stay free for new arrivals
 
     def __init__(self, files, device=0, max_units=48, range_slots=64):
-        # template slots + unit slots; a unit spreads over one or more range slots
         nf = len(files)
         self.batch = Batch(device, max_jobs=nf + max_units, range_slots=range_slots)
-        self.templates = []
+        self.templates, self.cost = [], {}
         for seqs in files:
             t = self.batch.add(seqs, 3, 3)        # p0 == p1: resident template, never runs
             assert t is not None
             self.templates.append(t)
+            self.cost[t] = cost_per_prime(self.batch.job_info(t)[0], seqs.kcount, seqs.nmax - seqs.nmin + 1)
         self.max_units = max_units
+        self.rate = None                          # cost units per second, measured
 
     def close(self):
         self.batch.close()
+
+    def _budgets(self, active, remaining):
+        """Shortest remaining first: primes per unit for the next round."""
+        def left(slot):
+            u = active[slot]
+            return remaining[slot] / math.log(max(u.p0, 3)) * self.cost[self.templates[u.file]]
+        order = sorted(active, key=left)
+        if self.rate is None:                     # first round: full windows
+            for slot in order:
+                self.batch.set_budget(slot, 1 << 40)
+            return
+        budget = self.rate * self.ROUND_S
+        for slot in order:
+            c = self.cost[self.templates[active[slot].file]]
+            want = left(slot)
+            give = min(want, budget)
+            budget -= give
+            self.batch.set_budget(slot, int(math.ceil(give / c)) if give > 0 else 0)
 
     def run(self, units, clock=time.perf_counter, collect_bitmaps=False):
         """Serve the units (sorted by arrival time); returns them with timings filled."""
         pending = sorted(units, key=lambda u: u.arrival)
         queue, active = [], {}
+        remaining = {}
         t0 = clock()
         i = 0
         while i < len(pending) or queue or active:
@@ -74,12 +112,13 @@ class Server:
                 if free == 0:
                     break
                 est = (u.p1 - u.p0) / math.log(max(u.p0, 3))
-                nsplit = max(1, min(free, math.ceil(est / self.PRIMES_PER_SLOT_ROUND)))
+                nsplit = max(1, min(free, self.MAX_SPLIT, math.ceil(est / self.PRIMES_PER_SLOT_ROUND)))
                 slot = self.batch.add_clone(self.templates[u.file], u.p0, u.p1, nsplit)
                 if slot is None:
                     break
                 u.admitted = clock() - t0
                 active[slot] = u
+                remaining[slot] = u.p1 - u.p0
                 queue.pop(0)
             if not active:
                 if i < len(pending):                 # idle until the next arrival
@@ -87,14 +126,24 @@ class Server:
                     if wait > 0:
                         time.sleep(wait)
                 continue
-            self.batch.run(1)                        # one round for every admitted unit
+            self._budgets(active, remaining)
+            _, before, _ = self.batch.poll()
+            r0 = clock()
+            self.batch.run(1)                        # one round for every unit with a budget
+            dt = clock() - r0
+            done, primes, rem = self.batch.poll()
+            work = sum(float(primes[s] - before[s]) * self.cost[self.templates[active[s].file]] for s in active)
+            if dt > 0 and work > 0:
+                r = work / dt
+                self.rate = r if self.rate is None else 0.7 * self.rate + 0.3 * r
             for slot in list(active):
-                q, primes, done = self.batch.job_info(slot)
-                if not done:
+                remaining[slot] = int(rem[slot])
+                if not done[slot]:
                     continue
                 u = active.pop(slot)
+                remaining.pop(slot)
                 u.finished = clock() - t0
-                u.primes = primes
+                u.primes = int(primes[slot])
                 u.factors = self.batch.factors(slot)
                 if collect_bitmaps:
                     u.bitmap = self.batch.bitmap(slot)
