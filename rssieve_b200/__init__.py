@@ -397,7 +397,9 @@ class Batch:
         nsplit range slots; None when no slot is free."""
         j = C.c_uint32(0)
         rc = lib().rs_batch_add_clone(self._b, src, p0, p1, nsplit, C.byref(j))
+        self.last_rc = rc
         if rc in (RS_EBUSY, RS_ENOMEM):
+            self.last_error = lib().rs_last_error().decode()
             return None
         _check(rc, "rs_batch_add_clone")
         self._seqs[j.value] = self._seqs[src]

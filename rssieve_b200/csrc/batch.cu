@@ -9,8 +9,8 @@
 //
 //   k_batch_windows  next window of every range (sized for ~0.6*RCAP primes)
 //   k_sieve_batch    segmented sieve, blockIdx.y = range
-//   k_mr_batch       Miller-Rabin, blockIdx.y = range
-//   k_setup_*<true>  per-prime set-up, blockIdx.y = range
+//   k_mr_batch       Miller-Rabin over the survivors of every range at once
+//   k_setup_*<true>  per-prime set-up over the primes of every range at once
 //   per (geometry, product) group: prefix of the group's prime counts, then one
 //   persistent k_bsgs<..., true> over all primes of the group's ranges (each
 //   prime carries its job index and loads that job's arguments)
@@ -32,8 +32,9 @@
 // next one, so the batch also serves a stream of arriving work units.  The
 // ten BSGS groups (geometry x product) cover every range slot and count only
 // the slots currently in them, so the captured round never changes.  A job's
-// bitmap and factor list come from the stream-ordered allocator, so admitting
-// or releasing a job does not synchronise the device.
+// bitmap and factor list come from the batch's own stream-ordered memory pool,
+// which keeps freed blocks mapped: admitting or releasing a job neither
+// synchronises the device nor maps new pages.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -94,6 +95,7 @@ struct rs_batch {
     std::vector<char> range_done;          // from the last rs_batch_poll
     bool win_dirty = false;
     u32 *d_win = nullptr;
+    u32 *d_prefix_c = nullptr, *d_prefix_p = nullptr;   // prefix sums over all ranges: survivors, primes
     u32 *h_win_pin = nullptr;
     std::vector<Group> groups;
     // device tables
@@ -119,6 +121,7 @@ struct rs_batch {
     u32 *h_pin = nullptr;       // [0] error word, [1] unfinished ranges, [2] factor count
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    cudaMemPool_t pool = nullptr;          // jobs' bitmaps and factor lists; keeps freed memory mapped
     u64 rounds = 0;
     bool done = false;
 };
@@ -144,13 +147,14 @@ extern "C" void rs_batch_destroy(rs_batch *b)
         if (j.d_factors) cudaFreeAsync(j.d_factors, b->stream);
     }
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->pool) cudaMemPoolDestroy(b->pool);
     for (auto &g : b->groups) {
         cudaFree(g.d_prefix);
         cudaFree(g.d_work);
     }
     void *ptrs[] = {b->d_sp, b->d_jobs, b->d_geoms, b->d_args, b->d_fctrs, b->d_ranges, b->d_wins, b->d_ctrs,
                     b->d_range_primes, b->d_cands, b->d_primes, b->d_hdr, b->d_aux, b->d_tabs, b->d_tgt, b->d_meta,
-                    b->d_err, b->d_stats, b->d_unfinished, b->d_win};
+                    b->d_err, b->d_stats, b->d_unfinished, b->d_win, b->d_prefix_c, b->d_prefix_p};
     for (void *p : ptrs) cudaFree(p);
     if (b->h_pin) cudaFreeHost(b->h_pin);
     if (b->h_win_pin) cudaFreeHost(b->h_win_pin);
@@ -207,6 +211,7 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         !alloc((void **)&b->d_tabs, (size_t)R * RCAP * TABS * 8) ||
         !alloc((void **)&b->d_tgt, (size_t)R * RCAP * KSTRIDE * 8) ||
         !alloc((void **)&b->d_meta, (size_t)R * RCAP * KSTRIDE) || !alloc((void **)&b->d_win, R * 4) ||
+        !alloc((void **)&b->d_prefix_c, (R + 1) * 4) || !alloc((void **)&b->d_prefix_p, (R + 1) * 4) ||
         cudaMallocHost(&b->h_pin, 16) != cudaSuccess || cudaMallocHost(&b->h_win_pin, R * 4) != cudaSuccess) {
         rs_set_error("cannot allocate a batch of %u range slots (about %zu MB)", R,
                      (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 9 + 24 + 8 + 16) >> 20);
@@ -224,6 +229,19 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
     if (bsgs_prepare() != cudaSuccess) {
         rs_set_error("cannot configure the BSGS kernels' shared memory");
         return fail(RS_ECUDA);
+    }
+    {
+        // a pool of our own whose freed blocks stay mapped: admitting a job after
+        // releasing one reuses memory instead of mapping new pages at every sync
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&b->pool, &props) != cudaSuccess) return fail(RS_ECUDA);
+        uint64_t keep = ~0ull;
+        if (cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+            return fail(RS_ECUDA);
     }
     for (int g = 0; g < NGEOM; ++g)
         for (int m = 0; m < 2; ++m) {
@@ -320,8 +338,9 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
         J.factor_cap = src->factor_cap;
     }
     const u32 fcap = tmpl ? 1u : J.factor_cap;       // a template never claims; its clones get factor_cap
-    if (cudaMallocAsync((void **)&J.d_bitmap, J.bitmap_words * 4, b->stream) != cudaSuccess ||
-        cudaMallocAsync((void **)&J.d_factors, (size_t)fcap * sizeof(FactorRec), b->stream) != cudaSuccess) {
+    if (cudaMallocFromPoolAsync((void **)&J.d_bitmap, J.bitmap_words * 4, b->pool, b->stream) != cudaSuccess ||
+        cudaMallocFromPoolAsync((void **)&J.d_factors, (size_t)fcap * sizeof(FactorRec), b->pool, b->stream) !=
+            cudaSuccess) {
         if (J.d_bitmap) cudaFreeAsync(J.d_bitmap, b->stream);
         if (J.d_factors) cudaFreeAsync(J.d_factors, b->stream);
         J = BJob();
@@ -432,9 +451,11 @@ static int batch_round(rs_batch *b)
     BCU(cudaMemsetAsync(b->d_unfinished, 0, 4, st));
     BCU(launch_batch_windows(b->d_ranges, b->d_wins, b->d_win, R, RCAP, b->d_ctrs, st));
     BCU(launch_sieve_batch(b->d_wins, R, max_blocks, b->d_sp, b->nsp, b->d_cands, CCAP, b->d_ctrs, b->d_err, st));
-    BCU(launch_mr_batch(b->d_cands, CCAP, b->d_primes, RCAP, b->d_ctrs, R, b->d_err, b->sms, st));
-    BCU(launch_setup_batch(b->d_jobs, b->d_geoms, b->d_ranges, b->d_primes, RCAP, b->d_ctrs, R, b->d_hdr, b->d_aux,
-                           b->d_tabs, b->d_tgt, b->d_meta, b->d_stats, st));
+    BCU(launch_batch_prefix_all(b->d_ranges, R, 0, CCAP, b->d_ctrs, b->d_prefix_c, st));
+    BCU(launch_mr_batch(b->d_cands, CCAP, b->d_primes, RCAP, b->d_ctrs, R, b->d_prefix_c, b->d_err, b->sms, st));
+    BCU(launch_batch_prefix_all(b->d_ranges, R, 1, RCAP, b->d_ctrs, b->d_prefix_p, st));
+    BCU(launch_setup_batch(b->d_jobs, b->d_geoms, b->d_ranges, b->d_primes, RCAP, b->d_prefix_p, R, b->d_hdr,
+                           b->d_aux, b->d_tabs, b->d_tgt, b->d_meta, b->d_stats, b->sms, st));
     BsgsArgs a;
     memset(&a, 0, sizeof a);
     a.stats = b->d_stats;

@@ -377,12 +377,8 @@ __device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
 // k*rcap + (0, 1, ...).
 __device__ __forceinline__ u32 batch_slot(u32 i, u32 nr, const u32 *prefix, u32 rcap)
 {
-    u32 lo = 0, hi = nr;                 // last k with prefix[k] <= i (prefix[k+1] > i then)
-    while (hi - lo > 1) {
-        const u32 mid = (lo + hi) >> 1;
-        if (prefix[mid] <= i) lo = mid; else hi = mid;
-    }
-    return lo * rcap + (i - prefix[lo]);
+    const u32 k = prefix_find(prefix, nr, i);
+    return k * rcap + (i - prefix[k]);
 }
 
 // MODE: 1 = every prime below 2^63 (Shoup giant steps), 0 = every prime at or
@@ -675,16 +671,36 @@ cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs,
 #undef RS_BSGS_CASE
 }
 
-// prefix[0] = 0, prefix[k+1] = prefix[k] + primes of range slot k when it is
-// active and in the (geom, shoup) group, else + 0 (one thread; nr is small)
-__global__ void k_batch_prefix(const BatchRange *ranges, u32 nr, int geom, int shoup, const u32 *ctrs, u32 rcap,
-                               u32 *prefix)
+// prefix[0] = 0, prefix[k+1] = prefix[k] + counter `which` of range slot k
+// (capped at rcap) when it is active and in the (geom, shoup) group -- or, for
+// geom < 0, when it is active -- else + 0.  One block of 256 threads: each
+// sums a contiguous run of slots, a block scan offsets the runs.
+__global__ void __launch_bounds__(256) k_batch_prefix(const BatchRange *ranges, u32 nr, int geom, int shoup,
+                                                      const u32 *ctrs, u32 rcap, u32 *prefix, int which)
 {
-    u32 acc = 0;
-    prefix[0] = 0;
-    for (u32 k = 0; k < nr; ++k) {
+    __shared__ u32 part[256];
+    const u32 t = threadIdx.x;
+    const u32 per = (nr + 255) / 256;
+    const u32 k0 = t * per, k1 = min(k0 + per, nr);
+    auto cnt = [&](u32 k) -> u32 {
         const BatchRange R = ranges[k];
-        if (R.active && R.geom == geom && R.shoup == shoup) acc += min(ctrs[k * BR_CTRS + 1], rcap);
+        const bool in = R.active && (geom < 0 || (R.geom == geom && R.shoup == shoup));
+        return in ? min(ctrs[k * BR_CTRS + which], rcap) : 0u;
+    };
+    u32 sum = 0;
+    for (u32 k = k0; k < k1; ++k) sum += cnt(k);
+    part[t] = sum;
+    __syncthreads();
+    for (u32 o = 1; o < 256; o <<= 1) {           // inclusive Hillis-Steele scan
+        const u32 v = (t >= o) ? part[t - o] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    u32 acc = part[t] - sum;                      // exclusive prefix of this run
+    if (t == 0) prefix[0] = 0;
+    for (u32 k = k0; k < k1; ++k) {
+        acc += cnt(k);
         prefix[k + 1] = acc;
     }
 }
@@ -692,7 +708,14 @@ __global__ void k_batch_prefix(const BatchRange *ranges, u32 nr, int geom, int s
 cudaError_t launch_batch_prefix(const BatchRange *ranges, u32 nr, int geom, bool shoup, const u32 *ctrs, u32 rcap,
                                 u32 *prefix, cudaStream_t st)
 {
-    k_batch_prefix<<<1, 1, 0, st>>>(ranges, nr, geom, shoup ? 1 : 0, ctrs, rcap, prefix);
+    k_batch_prefix<<<1, 256, 0, st>>>(ranges, nr, geom, shoup ? 1 : 0, ctrs, rcap, prefix, 1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_prefix_all(const BatchRange *ranges, u32 nr, int which, u32 cap, const u32 *ctrs,
+                                    u32 *prefix, cudaStream_t st)
+{
+    k_batch_prefix<<<1, 256, 0, st>>>(ranges, nr, -1, 0, ctrs, cap, prefix, which);
     return cudaGetLastError();
 }
 

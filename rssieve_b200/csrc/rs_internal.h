@@ -160,6 +160,18 @@ struct JobGeom {
     u32 q, c, tpb, m1, m2, pad_;
 };
 
+// Index i of work spread over nr ranges with prefix sums prefix[0..nr]:
+// the range k with prefix[k] <= i < prefix[k+1] (i < prefix[nr]).
+__device__ __forceinline__ u32 prefix_find(const u32 *prefix, u32 nr, u32 i)
+{
+    u32 lo = 0, hi = nr;
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (prefix[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 // launch wrappers (sieve.cu, setup.cu, bsgs.cu)
 cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp, u64 *cands, u32 cand_cap,
                          u32 *ctrs, u32 *err, cudaStream_t st);
@@ -182,15 +194,21 @@ cudaError_t launch_batch_windows(BatchRange *ranges, BatchWin *wins, const u32 *
                                  cudaStream_t st);
 cudaError_t launch_sieve_batch(const BatchWin *wins, u32 nranges, u32 max_blocks, const u32 *sp, u32 nsp, u64 *cands,
                                u32 ccap, u32 *ctrs, u32 *err, cudaStream_t st);
-cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges, u32 *err,
-                            int sms, cudaStream_t st);
+// Miller-Rabin over the survivors of all ranges (prefix_c: their counts'
+// prefix sums); primes go to their range's slots
+cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges,
+                            const u32 *prefix_c, u32 *err, int sms, cudaStream_t st);
+// set-up of the primes of all ranges (prefix_p: prefix sums of their counts)
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
-                               u32 rcap, const u32 *ctrs, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs, u64 *tgt,
-                               unsigned char *meta, u64 *stats, cudaStream_t st);
+                               u32 rcap, const u32 *prefix_p, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs,
+                               u64 *tgt, unsigned char *meta, u64 *stats, int sms, cudaStream_t st);
 // one BSGS launch per (geometry, mode) group over range slots [0, nr): prefix
 // (nr+1 entries) counts the primes of the active slots of that group only
 cudaError_t launch_batch_prefix(const BatchRange *ranges, u32 nr, int geom, bool shoup, const u32 *ctrs, u32 rcap,
                                 u32 *prefix, cudaStream_t st);
+// prefix over every active range of counter `which` (0: survivors, 1: primes), each capped at cap
+cudaError_t launch_batch_prefix_all(const BatchRange *ranges, u32 nr, int which, u32 cap, const u32 *ctrs,
+                                    u32 *prefix, cudaStream_t st);
 cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
                               const u64 *tgt, const unsigned char *meta, u32 nr, const u32 *prefix, u32 rcap,
                               u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st);

@@ -62,35 +62,11 @@ struct PrimeAux {        // kernel 1 -> kernel 2 scalars
     u32 pad_;
 };
 
-// Kernel 1.  Single job: primes[first, first+count) into records [0, count)
-// with the launch's geometry gm.  Batch (BATCH): blockIdx.y is the range; its
-// job, geometry, prime count and record slots come from the batch tables.
-template <bool BATCH>
-__global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ jobs, const u64 *__restrict__ primes,
-                                                     u32 first, u32 count, PrimeHdr *__restrict__ hdr,
-                                                     PrimeAux *__restrict__ aux, u64 *__restrict__ tabs, JobGeom gm,
-                                                     const JobGeom *__restrict__ geoms,
-                                                     const BatchRange *__restrict__ ranges,
-                                                     const u32 *__restrict__ ctrs, u32 rcap)
+// Per-prime constants of prime p into record t.
+__device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, u64 p, u32 t, u32 jb,
+                                                PrimeHdr *__restrict__ hdr, PrimeAux *__restrict__ aux,
+                                                u64 *__restrict__ tabs, const JobGeom &gm)
 {
-    const JobDev *job = jobs;
-    u32 jb = 0;
-    if (BATCH) {
-        const u32 r = blockIdx.y;
-        jb = ranges[r].job;
-        job = jobs + jb;
-        gm = geoms[jb];
-        count = min(ctrs[r * BR_CTRS + 1], rcap);
-        const size_t off = (size_t)r * rcap;
-        primes += off;
-        hdr += off;
-        aux += off;
-        tabs += off * TABS;
-        first = 0;
-    }
-    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const u64 p = primes[first + t];
     PrimeHdr H;
     H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.job = jb;
     H.Sh = 0; H.Sw = 0;
@@ -133,33 +109,40 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
     aux[t] = X;
 }
 
-// Kernel 2: one warp per prime; lanes walk the sequences.  BATCH as kernel 1.
+
+// Kernel 1.  Single job: primes[first, first+count) into records [0, count)
+// with the launch's geometry gm.  Batch (BATCH): the primes of every range as
+// one index space (prefix: prefix sums of the ranges' prime counts); prime i
+// of range r is record r*rcap + i, with its job's sequences and geometry.
 template <bool BATCH>
-__global__ void __launch_bounds__(SETUP_TPB, 6) k_setup_k(const JobDev *__restrict__ jobs, PrimeHdr *__restrict__ hdr,
-                                                       const PrimeAux *__restrict__ aux, u32 count,
-                                                       u64 *__restrict__ tabs, u64 *__restrict__ tgt,
-                                                       unsigned char *__restrict__ meta, u64 *__restrict__ stats,
-                                                       JobGeom gm, const JobGeom *__restrict__ geoms,
-                                                       const BatchRange *__restrict__ ranges,
-                                                       const u32 *__restrict__ ctrs, u32 rcap)
+__global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ jobs, const u64 *__restrict__ primes,
+                                                     u32 first, u32 count, PrimeHdr *__restrict__ hdr,
+                                                     PrimeAux *__restrict__ aux, u64 *__restrict__ tabs, JobGeom gm,
+                                                     const JobGeom *__restrict__ geoms,
+                                                     const BatchRange *__restrict__ ranges,
+                                                     const u32 *__restrict__ prefix, u32 nr, u32 rcap)
 {
-    const JobDev *job = jobs;
+    const u32 stride = gridDim.x * blockDim.x;
     if (BATCH) {
-        const u32 r = blockIdx.y;
-        const u32 jb = ranges[r].job;
-        job = jobs + jb;
-        gm = geoms[jb];
-        count = min(ctrs[r * BR_CTRS + 1], rcap);
-        const size_t off = (size_t)r * rcap;
-        hdr += off;
-        aux += off;
-        tabs += off * TABS;
-        tgt += off * KSTRIDE;
-        meta += off * KSTRIDE;
+        const u32 total = prefix[nr];
+        for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+            const u32 r = prefix_find(prefix, nr, i);
+            const u32 rec = r * rcap + (i - prefix[r]);
+            const u32 jb = ranges[r].job;
+            setup_prime_one(jobs + jb, primes[rec], rec, jb, hdr, aux, tabs, geoms[jb]);
+        }
+        return;
     }
-    const u32 lane = threadIdx.x & 31;
-    const u32 w = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5;
-    if (w >= count) return;
+    for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += stride)
+        setup_prime_one(jobs, primes[first + t], t, 0, hdr, aux, tabs, gm);
+}
+
+// Sequence classes, targets and giant-step tables of record w (one warp).
+__device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 w, u32 lane, PrimeHdr *__restrict__ hdr,
+                                            const PrimeAux *__restrict__ aux, u64 *__restrict__ tabs,
+                                            u64 *__restrict__ tgt, unsigned char *__restrict__ meta,
+                                            u64 *__restrict__ stats, const JobGeom &gm)
+{
     PrimeHdr H = hdr[w];
     if (H.p == 0) {
         if (lane == 0) atomicAdd(&stats[ST_SKIPPED], 1ull);
@@ -261,6 +244,34 @@ __global__ void __launch_bounds__(SETUP_TPB, 6) k_setup_k(const JobDev *__restri
     }
 }
 
+
+// Kernel 2: one warp per prime; lanes walk the sequences.  BATCH as kernel 1.
+template <bool BATCH>
+__global__ void __launch_bounds__(SETUP_TPB, 6) k_setup_k(const JobDev *__restrict__ jobs, PrimeHdr *__restrict__ hdr,
+                                                       const PrimeAux *__restrict__ aux, u32 count,
+                                                       u64 *__restrict__ tabs, u64 *__restrict__ tgt,
+                                                       unsigned char *__restrict__ meta, u64 *__restrict__ stats,
+                                                       JobGeom gm, const JobGeom *__restrict__ geoms,
+                                                       const BatchRange *__restrict__ ranges,
+                                                       const u32 *__restrict__ prefix, u32 nr, u32 rcap)
+{
+    const u32 lane = threadIdx.x & 31;
+    const u32 nwarps = gridDim.x * (SETUP_TPB / 32);
+    // w is uniform over the warp, so the warp-wide ballots of a prime stay whole
+    if (BATCH) {
+        const u32 total = prefix[nr];
+        for (u32 i = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5; i < total; i += nwarps) {
+            const u32 r = prefix_find(prefix, nr, i);
+            const u32 rec = r * rcap + (i - prefix[r]);
+            const u32 jb = ranges[r].job;
+            setup_k_one(jobs + jb, rec, lane, hdr, aux, tabs, tgt, meta, stats, geoms[jb]);
+        }
+        return;
+    }
+    for (u32 w = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5; w < count; w += nwarps)
+        setup_k_one(jobs, w, lane, hdr, aux, tabs, tgt, meta, stats, gm);
+}
+
 cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 count, PrimeHdr *hdr, void *aux, u64 *tabs,
                          u64 *tgt, unsigned char *meta, u64 *stats, int geom, u32 L, cudaStream_t st)
 {
@@ -271,27 +282,27 @@ cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 co
     gm.m1 = (u32)(((u64)L + g.q - 1) / g.q);
     gm.m2 = (u32)(((u64)L + 2ull * g.q - 1) / (2ull * g.q));
     k_setup_prime<false><<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, tabs, gm,
-                                                              nullptr, nullptr, nullptr, 0);
+                                                              nullptr, nullptr, nullptr, 0, 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const u32 wpb = SETUP_TPB / 32;
     k_setup_k<false><<<(count + wpb - 1) / wpb, SETUP_TPB, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, tgt,
-                                                                   meta, stats, gm, nullptr, nullptr, nullptr, 0);
+                                                                   meta, stats, gm, nullptr, nullptr, nullptr, 0, 0);
     return cudaGetLastError();
 }
 
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
-                               u32 rcap, const u32 *ctrs, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs, u64 *tgt,
-                               unsigned char *meta, u64 *stats, cudaStream_t st)
+                               u32 rcap, const u32 *prefix_p, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs,
+                               u64 *tgt, unsigned char *meta, u64 *stats, int sms, cudaStream_t st)
 {
     JobGeom gm{};
-    k_setup_prime<true><<<dim3((rcap + 255) / 256, nranges), 256, 0, st>>>(jobs, primes, 0, 0, hdr, (PrimeAux *)aux,
-                                                                           tabs, gm, geoms, ranges, ctrs, rcap);
+    // full-device grids; the kernels stride over the primes of every range
+    k_setup_prime<true><<<sms * 4, 256, 0, st>>>(jobs, primes, 0, 0, hdr, (PrimeAux *)aux, tabs, gm, geoms, ranges,
+                                                 prefix_p, nranges, rcap);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    const u32 wpb = SETUP_TPB / 32;
-    k_setup_k<true><<<dim3((rcap + wpb - 1) / wpb, nranges), SETUP_TPB, 0, st>>>(
-        jobs, hdr, (const PrimeAux *)aux, 0, tabs, tgt, meta, stats, gm, geoms, ranges, ctrs, rcap);
+    k_setup_k<true><<<sms * 6, SETUP_TPB, 0, st>>>(jobs, hdr, (const PrimeAux *)aux, 0, tabs, tgt, meta, stats, gm,
+                                                   geoms, ranges, prefix_p, nranges, rcap);
     return cudaGetLastError();
 }
 

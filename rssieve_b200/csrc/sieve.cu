@@ -195,13 +195,22 @@ __global__ void __launch_bounds__(256) k_mr(const u64 *__restrict__ cands, const
     mr_list(cands, ctrs, cand_cap, primes, prime_cap, prime_ctr, err);
 }
 
-// Batch round: blockIdx.y is the range.
+// Batch round: the survivors of every range as one index space (prefix_c:
+// prefix sums of their counts), so a few active ranges still fill the device;
+// each prime takes a slot of its range with one atomic.
 __global__ void __launch_bounds__(256) k_mr_batch(const u64 *__restrict__ cands, u32 ccap, u64 *__restrict__ primes,
-                                                  u32 rcap, u32 *ctrs, u32 *err)
+                                                  u32 rcap, u32 *ctrs, const u32 *__restrict__ prefix_c, u32 nr,
+                                                  u32 *err)
 {
-    const u32 r = blockIdx.y;
-    mr_list(cands + (size_t)r * ccap, ctrs + r * BR_CTRS, ccap, primes + (size_t)r * rcap, rcap,
-            ctrs + r * BR_CTRS + 1, err);
+    const u32 total = prefix_c[nr];
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const u32 r = prefix_find(prefix_c, nr, i);
+        const u64 v = cands[(size_t)r * ccap + (i - prefix_c[r])];
+        if (!is_prime_mr(v)) continue;
+        const u32 pos = atomicAdd(&ctrs[r * BR_CTRS + 1], 1u);
+        if (pos < rcap) primes[(size_t)r * rcap + pos] = v;
+        else atomicOr(err, ERR_PRIME_OVERFLOW);
+    }
 }
 
 // Next window of every range, sized for win[r] primes (width win*ln p, at
@@ -256,12 +265,10 @@ cudaError_t launch_sieve_batch(const BatchWin *wins, u32 nranges, u32 max_blocks
     return cudaGetLastError();
 }
 
-cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges, u32 *err,
-                            int sms, cudaStream_t st)
+cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges,
+                            const u32 *prefix_c, u32 *err, int sms, cudaStream_t st)
 {
-    unsigned bx = (unsigned)((sms * 8 + nranges - 1) / nranges);
-    if (bx < 2) bx = 2;
-    k_mr_batch<<<dim3(bx, nranges), 256, 0, st>>>(cands, ccap, primes, rcap, ctrs, err);
+    k_mr_batch<<<sms * 8, 256, 0, st>>>(cands, ccap, primes, rcap, ctrs, prefix_c, nranges, err);
     return cudaGetLastError();
 }
 

@@ -56,10 +56,10 @@ class Server:
 
     PRIMES_PER_SLOT_ROUND = 0.6 * 65536    # one range slot's round capacity
     ROUND_S = 0.006                        # target round duration
-    MAX_SPLIT = 8                          # range slots per unit: a few absorb a round's budget,
+    MAX_SPLIT = 4                          # range slots per unit: a few absorb a round's budget,
                                            # the rest stay free for new arrivals
 
-    def __init__(self, files, device=0, max_units=48, range_slots=64):
+    def __init__(self, files, device=0, max_units=48, range_slots=128):
         nf = len(files)
         self.batch = Batch(device, max_jobs=nf + max_units, range_slots=range_slots)
         self.templates, self.cost = [], {}
@@ -74,29 +74,33 @@ class Server:
     def close(self):
         self.batch.close()
 
-    def _budgets(self, active, remaining):
-        """Shortest remaining first: primes per unit for the next round."""
+    def _budgets(self, active, remaining, given):
+        """Shortest remaining first: primes per unit for the next round (calls the
+        library only where a unit's budget changes)."""
         def left(slot):
             u = active[slot]
             return remaining[slot] / math.log(max(u.p0, 3)) * self.cost[self.templates[u.file]]
         order = sorted(active, key=left)
-        if self.rate is None:                     # first round: full windows
-            for slot in order:
-                self.batch.set_budget(slot, 1 << 40)
-            return
-        budget = self.rate * self.ROUND_S
+        budget = None if self.rate is None else self.rate * self.ROUND_S
         for slot in order:
-            c = self.cost[self.templates[active[slot].file]]
-            want = left(slot)
-            give = min(want, budget)
-            budget -= give
-            self.batch.set_budget(slot, int(math.ceil(give / c)) if give > 0 else 0)
+            if budget is None:                    # first round: full windows
+                n = 1 << 40
+            else:
+                c = self.cost[self.templates[active[slot].file]]
+                give = min(left(slot), budget)
+                budget -= give
+                n = int(math.ceil(give / c)) if give > 0 else 0
+            if given.get(slot) != n:
+                self.batch.set_budget(slot, n)
+                given[slot] = n
 
-    def run(self, units, clock=time.perf_counter, collect_bitmaps=False):
-        """Serve the units (sorted by arrival time); returns them with timings filled."""
+    def run(self, units, clock=time.perf_counter, collect_bitmaps=False, trace=None):
+        """Serve the units (sorted by arrival time); returns them with timings filled.
+        trace: an optional list that receives one record per round."""
         pending = sorted(units, key=lambda u: u.arrival)
         queue, active = [], {}
-        remaining = {}
+        remaining, given = {}, {}
+        primes_seen = {}
         t0 = clock()
         i = 0
         while i < len(pending) or queue or active:
@@ -119,6 +123,8 @@ class Server:
                 u.admitted = clock() - t0
                 active[slot] = u
                 remaining[slot] = u.p1 - u.p0
+                primes_seen[slot] = 0
+                given.pop(slot, None)
                 queue.pop(0)
             if not active:
                 if i < len(pending):                 # idle until the next arrival
@@ -126,22 +132,29 @@ class Server:
                     if wait > 0:
                         time.sleep(wait)
                 continue
-            self._budgets(active, remaining)
-            _, before, _ = self.batch.poll()
+            self._budgets(active, remaining, given)
             r0 = clock()
             self.batch.run(1)                        # one round for every unit with a budget
-            dt = clock() - r0
             done, primes, rem = self.batch.poll()
-            work = sum(float(primes[s] - before[s]) * self.cost[self.templates[active[s].file]] for s in active)
+            dt = clock() - r0
+            work = sum(float(primes[s] - primes_seen[s]) * self.cost[self.templates[active[s].file]] for s in active)
+            if trace is not None:
+                trace.append({"t": r0 - t0, "dt": dt, "rate": self.rate, "work": work, "queue": len(queue),
+                              "free": self.batch.free_slots(),
+                              "units": {active[s].uid: (given.get(s), int(primes[s] - primes_seen[s]), int(rem[s]))
+                                        for s in active}})
             if dt > 0 and work > 0:
                 r = work / dt
                 self.rate = r if self.rate is None else 0.7 * self.rate + 0.3 * r
             for slot in list(active):
                 remaining[slot] = int(rem[slot])
+                primes_seen[slot] = int(primes[slot])
                 if not done[slot]:
                     continue
                 u = active.pop(slot)
                 remaining.pop(slot)
+                primes_seen.pop(slot)
+                given.pop(slot, None)
                 u.finished = clock() - t0
                 u.primes = int(primes[slot])
                 u.factors = self.batch.factors(slot)
