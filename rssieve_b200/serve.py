@@ -56,11 +56,14 @@ class Server:
 
     PRIMES_PER_SLOT_ROUND = 0.6 * 65536    # one range slot's round capacity
     ROUND_S = 0.006                        # target round duration
+    MIN_ROUND_S = 0.0015                   # shortest round when a unit is about to finish
     MAX_SPLIT = 4                          # range slots per unit: a few absorb a round's budget,
                                            # the rest stay free for new arrivals
 
-    def __init__(self, files, device=0, max_units=48, range_slots=128):
+    def __init__(self, files, device=0, max_units=48, range_slots=128, round_s=None, short_rounds=True):
         nf = len(files)
+        self.round_s = round_s or self.ROUND_S
+        self.short_rounds = short_rounds
         self.batch = Batch(device, max_jobs=nf + max_units, range_slots=range_slots)
         self.templates, self.cost = [], {}
         for seqs in files:
@@ -81,7 +84,13 @@ class Server:
             u = active[slot]
             return remaining[slot] / math.log(max(u.p0, 3)) * self.cost[self.templates[u.file]]
         order = sorted(active, key=left)
-        budget = None if self.rate is None else self.rate * self.ROUND_S
+        budget = None if self.rate is None else self.rate * self.round_s
+        if budget is not None and self.short_rounds and order:
+            # a unit that finishes this round shares it with at most as much other work
+            # as its own, so the round ends within twice the time the unit needs alone
+            first = left(order[0])
+            if first < budget:
+                budget = max(2.0 * first, self.rate * self.MIN_ROUND_S)
         for slot in order:
             if budget is None:                    # first round: full windows
                 n = 1 << 40

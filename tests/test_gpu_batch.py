@@ -130,3 +130,52 @@ def test_clone_split_over_range_slots_matches_single_job_path(rs, sieve):
         assert b.free_slots() == (3, 8)
     finally:
         b.close()
+
+
+def test_batch_high_p_edge_matches_oracle(rs, oracle):
+    """Config-4 shape in the batch: b = 5, 20 sequences, k even below 2^40, c
+    alternating, p just below 2^64 (full-width Montgomery products), the window
+    cut over 5 range slots of a clone, beside a small-p job in the same rounds;
+    eliminated terms and bitmap equal to the brute-force oracle."""
+    job = W.small_job(24, kcount=20, base=5, nmin=1000, nmax=200000, keep=0.05, kmax=1 << 40)
+    small = W.small_job(59, kcount=6, base=2, nmin=1000, nmax=9000, keep=0.4, kmax=1 << 24)
+    p0, p1 = (1 << 64) - (1 << 22), (1 << 64) - 1
+    b = rs.Batch(0, max_jobs=4, range_slots=8)
+    try:
+        t = b.add(W.seqs_of(job), p0, p0)
+        j = b.add_clone(t, p0, p1, nsplit=5)
+        s = b.add(W.seqs_of(small), 3, 200_000)
+        assert b.run(0)
+        for jid, jb, lo, hi in ((j, job, p0, p1), (s, small, 3, 200_000)):
+            plist = oracle.primes(lo, hi)
+            ofac, _, obm = oracle.brute(oracle_job(oracle, jb), plist, ref_skip=True)
+            f = b.factors(jid)
+            assert _terms(f) == _terms(ofac), jb["name"]
+            assert np.array_equal(b.bitmap(jid), obm), jb["name"]
+            assert b.job_info(jid)[1:] == (len(plist), True)
+            for row in f[:500]:
+                sq = int(row["seq"])
+                assert rs.verify_factor(int(row["p"]), jb["k"][sq], int(row["n"]), jb["c"][sq], jb["base"]) == 1
+    finally:
+        b.close()
+
+
+def test_batch_config4_job_matches_single_job_path(rs, sieve):
+    """The config-4 job itself (n in [10^6, 3*10^6), p from 2^64 - 2^36) on a
+    2^24-wide window over 8 range slots: batch == single-job path."""
+    job = W.config4()
+    seqs = W.seqs_of(job)
+    p0 = job["prange"][0]
+    p1 = p0 + (1 << 24)
+    b = rs.Batch(0, max_jobs=2, range_slots=8)
+    try:
+        t = b.add(seqs, p0, p0)
+        j = b.add_clone(t, p0, p1, nsplit=8)
+        assert b.run(0)
+        sieve.load(seqs)
+        cnt = sieve.run(p0, p1)
+        assert _terms(b.factors(j)) == _terms(sieve.factors())
+        assert np.array_equal(b.bitmap(j), sieve.bitmap())
+        assert b.job_info(j)[1] == cnt["primes"]
+    finally:
+        b.close()
