@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--baby-steps", type=int, default=0, help="fix Q baby steps per prime (0: the per-job tuner)")
-    ap.add_argument("--no-forms", action="store_true", help="skip the batched (config 3) and served (config 5) forms")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the batched (configs 2, 3, 4) and served (config 5) forms")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     return ap.parse_args()
 
@@ -169,6 +170,52 @@ def measure_batched(torch, rs, W, seed=3, njobs=48, window_log2=24):
             "primes": int(batch_primes), "plain_primes_per_s": plain_primes / (pms / 1e3),
             "batched_primes_per_s": batch_primes / (bms / 1e3), "batched_over_plain": pms / bms,
             "identical_eliminated_terms": bool(same and plain_primes == batch_primes), "baby_steps_used": qs}
+
+
+def measure_one_job_batched(torch, rs, W, job, p0, width_log2, nsplit, label):
+    """One job over one p-window through the single-job path and through the batch
+    (a resident copy of the job cloned over nsplit range slots, at the Q the
+    single-job tuner measured for the job's shape); CUDA events on one side stream
+    bracket each, the batch's upload and clone included."""
+    import numpy as np
+    seqs = W.seqs_of(job)
+    p1 = p0 + (1 << width_log2)
+    st = torch.cuda.Stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    sv = rs.Sieve(torch.cuda.current_device())
+    sv.set_stream(st.cuda_stream)
+    sv.load(seqs)
+    sv.run(p0, p0 + (1 << 26))                 # warm: the tuner measures this job shape's Q
+    sv.load(seqs)
+    torch.cuda.synchronize()
+    ev[0].record(st)
+    plain_primes = sv.run(p0, p1)["primes"]
+    ev[1].record(st)
+    torch.cuda.synchronize()
+    f = sv.factors()
+    plain_terms = set(zip(f["seq"].tolist(), f["n"].tolist()))
+    plain_bm = sv.bitmap()
+    sv.close()
+    b = rs.Batch(torch.cuda.current_device(), max_jobs=2, range_slots=nsplit)
+    b.set_stream(st.cuda_stream)
+    torch.cuda.synchronize()
+    ev[2].record(st)
+    t = b.add(seqs, p0, p0)
+    j = b.add_clone(t, p0, p1, nsplit)
+    b.run(0)
+    ev[3].record(st)
+    torch.cuda.synchronize()
+    f = b.factors(j)
+    q, batch_primes, _ = b.job_info(j)
+    same = (set(zip(f["seq"].tolist(), f["n"].tolist())) == plain_terms and batch_primes == plain_primes
+            and np.array_equal(b.bitmap(j), plain_bm))
+    b.close()
+    pms, bms = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
+    return {"workload": "%s: one 2^%d-wide p-window from %s, batch over %d range slots" % (
+                label, width_log2, hex(p0), nsplit),
+            "primes": int(batch_primes), "plain_primes_per_s": plain_primes / (pms / 1e3),
+            "batched_primes_per_s": batch_primes / (bms / 1e3), "batched_over_plain": pms / bms,
+            "identical_eliminated_terms": bool(same), "baby_steps_used": q}
 
 
 def measure_served(rs, W, serve, seed=5, nunits=60, rate=8.0, width_log2=(22, 26)):
@@ -344,7 +391,12 @@ def main():
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         from rssieve_b200 import serve
-        forms = {"batched": measure_batched(torch, rs, W), "served": measure_served(rs, W, serve)}
+        forms = {"batched": measure_batched(torch, rs, W),
+                 "batched_config2": measure_one_job_batched(torch, rs, W, job, P_START + (1 << 37), 29, 32,
+                                                            "config2 job"),
+                 "batched_config4": measure_one_job_batched(torch, rs, W, W.config4(), (1 << 64) - (1 << 36), 30, 32,
+                                                            "config4 job (b=5, 20 seqs, k even < 2^40, p near 2^64)"),
+                 "served": measure_served(rs, W, serve)}
 
     if rank == 0:
         line = {

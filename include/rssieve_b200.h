@@ -221,6 +221,14 @@ int rs_batch_set_budget(rs_batch *b, uint32_t job, uint64_t primes);
 int rs_batch_poll(rs_batch *b, uint8_t *done, uint64_t *primes, uint64_t *remaining);
 /* Free job slots and range slots. */
 int rs_batch_free_slots(rs_batch *b, uint32_t *jobs, uint32_t *ranges);
+/* Device memory a job, or a clone of it, holds while admitted: its bitmap and
+ * a factor list with room for every candidate term. */
+int rs_batch_job_bytes(rs_batch *b, uint32_t job, uint64_t *bytes);
+/* Maps `bytes` of device memory into the batch's job pool ahead of time, so that
+ * later admissions up to that total reuse it instead of mapping new memory
+ * (which can take hundreds of milliseconds).  RS_ENOMEM when the device cannot
+ * provide it.  Serving loops admit units by footprint within this reserve. */
+int rs_batch_reserve(rs_batch *b, uint64_t bytes);
 /* Frees a job's slots (fetch its factors and bitmap first). */
 int rs_batch_release(rs_batch *b, uint32_t job);
 /* Runs up to max_rounds rounds (0: until every job is done, or every

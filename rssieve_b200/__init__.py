@@ -52,7 +52,8 @@ EXPORTS = (
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
     "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_primes_generate_noalloc",
     "rs_set_baby_steps", "rs_get_baby_steps",
-    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone", "rs_batch_free_slots", "rs_batch_release", "rs_batch_set_budget",
+    "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone",
+    "rs_batch_free_slots", "rs_batch_job_bytes", "rs_batch_reserve", "rs_batch_release", "rs_batch_set_budget",
     "rs_batch_poll", "rs_batch_run",
     "rs_batch_factors_fetch", "rs_batch_bitmap_download", "rs_batch_job_info", "rs_batch_counters",
 )
@@ -110,6 +111,8 @@ def lib():
         "rs_batch_release": (C.c_int, [vp, u32]),
         "rs_batch_add_clone": (C.c_int, [vp, u32, u64, u64, u32, C.POINTER(u32)]),
         "rs_batch_free_slots": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32)]),
+        "rs_batch_job_bytes": (C.c_int, [vp, u32, C.POINTER(C.c_uint64)]),
+        "rs_batch_reserve": (C.c_int, [vp, C.c_uint64]),
         "rs_batch_set_budget": (C.c_int, [vp, u32, u64]),
         "rs_batch_poll": (C.c_int, [vp, vp, vp, vp]),
         "rs_batch_destroy": (None, [vp]),
@@ -404,6 +407,20 @@ class Batch:
         _check(rc, "rs_batch_add_clone")
         self._seqs[j.value] = self._seqs[src]
         return j.value
+
+    def job_bytes(self, job):
+        """Device memory a job (or a clone of it) holds while admitted."""
+        n = C.c_uint64(0)
+        _check(lib().rs_batch_job_bytes(self._b, job, C.byref(n)), "rs_batch_job_bytes")
+        return n.value
+
+    def reserve(self, nbytes):
+        """Map nbytes into the batch's job pool ahead of admissions; False if the device lacks them."""
+        rc = lib().rs_batch_reserve(self._b, C.c_uint64(int(nbytes)))
+        if rc == RS_ENOMEM:
+            return False
+        _check(rc, "rs_batch_reserve")
+        return True
 
     def free_slots(self):
         """(free job slots, free range slots)."""

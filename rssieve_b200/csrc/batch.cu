@@ -22,8 +22,9 @@
 //
 // A job's p-range is split at 2^63 into two ranges (Shoup giant steps below,
 // Montgomery above) that share its bitmap and factor list.  Each job's BSGS
-// geometry comes from the per-prime cost model (geom_model_best) unless the
-// caller fixes Q.
+// geometry is the one a single-job run on the device measured for the job's
+// shape (base, sequence count, n-range), else the per-prime cost model's
+// (geom_model_best), unless the caller fixes Q.
 //
 // Capacity is fixed when the batch is created: job slots and range slots (each
 // range slot owns one round's buffers, about 136 MB).  Jobs can be added
@@ -33,7 +34,8 @@
 // ten BSGS groups (geometry x product) cover every range slot and count only
 // the slots currently in them, so the captured round never changes.  A job's
 // bitmap and factor list come from the batch's own stream-ordered memory pool,
-// which keeps freed blocks mapped: admitting or releasing a job neither
+// which keeps freed blocks mapped and can be grown ahead of time
+// (rs_batch_reserve): admitting or releasing a job neither
 // synchronises the device nor maps new pages.
 #include <algorithm>
 #include <cstring>
@@ -327,7 +329,12 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
     J = BJob();
     if (s) {
         jobdev_from_seqs(s, &J.jd);
-        J.geom = q ? geom_index(q) : geom_model_best(J.jd.kcount, J.jd.L);
+        if (q) {
+            J.geom = geom_index(q);
+        } else {        // measured by a single-job run of this shape on the device, else the model
+            const int known = tuned_geom_get(b->device, job_shape_key(J.jd.base, J.jd.kcount, J.jd.L));
+            J.geom = known >= 0 ? known : geom_model_best(J.jd.kcount, J.jd.L);
+        }
         J.bitmap_words = (size_t)s->kcount * s->words_per_seq;
         const uint64_t cand = rs_seqs_count(s);
         J.factor_cap = (u32)std::min<uint64_t>(cand + 1, 0xFFFFFFF0ull);
@@ -395,6 +402,29 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
     BCU(cudaStreamSynchronize(b->stream));     // the host structs above go out of scope
     b->done = false;
     if (job) *job = jid;
+    return RS_OK;
+}
+
+extern "C" int rs_batch_reserve(rs_batch *b, uint64_t bytes)
+{
+    if (!b) return RS_EARG;
+    BCU(cudaSetDevice(b->device));
+    void *p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, bytes, b->pool, b->stream) != cudaSuccess) {
+        cudaGetLastError();
+        rs_set_error("rs_batch_reserve: cannot map %llu bytes of device memory", (unsigned long long)bytes);
+        return RS_ENOMEM;
+    }
+    BCU(cudaFreeAsync(p, b->stream));
+    BCU(cudaStreamSynchronize(b->stream));
+    return RS_OK;
+}
+
+extern "C" int rs_batch_job_bytes(rs_batch *b, uint32_t job, uint64_t *bytes)
+{
+    if (!b || !bytes || job >= b->max_jobs || !b->jobs[job].used) return RS_EARG;
+    const BJob &J = b->jobs[job];
+    *bytes = (uint64_t)J.bitmap_words * 4 + (uint64_t)J.factor_cap * sizeof(FactorRec);
     return RS_OK;
 }
 

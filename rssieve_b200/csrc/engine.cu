@@ -9,7 +9,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "rs_internal.h"
@@ -58,7 +61,6 @@ struct rs_ctx {
     double tune_ms[NGEOM];
     u64 tune_primes[NGEOM];
     std::vector<int> chunk_geom;
-    std::vector<std::pair<u64, int>> tuned;   // job shape (base, kcount, L) -> tuned geometry
     // timing of the last rs_run_range
     std::vector<cudaEvent_t> ev;
     double last_bsgs_ms = 0, last_total_ms = 0;
@@ -140,7 +142,6 @@ extern "C" int rs_ctx_create(int device, rs_ctx **out)
     }
     rs_ctx *c = new rs_ctx();
     c->device = device;
-    int rc = RS_OK;
     auto fail = [&](int r) { rs_ctx_destroy(c); return r; };
     if (cudaSetDevice(device) != cudaSuccess) return fail((rs_set_error("cudaSetDevice failed"), RS_ECUDA));
     cudaDeviceProp prop;
@@ -176,7 +177,6 @@ extern "C" int rs_ctx_create(int device, rs_ctx **out)
         rs_set_error("BSGS kernel needs %zu B of shared memory", bsgs_smem_bytes(0));
         return fail(RS_ECUDA);
     }
-    (void)rc;
     *out = c;
     return RS_OK;
 }
@@ -195,10 +195,27 @@ static void odd_split(u64 x, u64 &odd, u32 &v2)
     odd = x;
 }
 
-// Jobs of one shape share a tuned geometry (a reloaded or resumed job skips tuning).
+// Jobs of one shape share a tuned geometry (a reloaded or resumed job skips
+// tuning), across every context and batch on the device.
+static std::mutex g_tuned_mu;
+static std::map<std::pair<int, u64>, int> g_tuned;
+
+int rs::tuned_geom_get(int device, u64 shape)
+{
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    auto it = g_tuned.find({device, shape});
+    return it == g_tuned.end() ? -1 : it->second;
+}
+
+void rs::tuned_geom_put(int device, u64 shape, int geom)
+{
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    g_tuned[{device, shape}] = geom;
+}
+
 static u64 job_shape(const rs_ctx *c)
 {
-    return ((u64)c->h_job.base << 40) ^ ((u64)c->h_job.kcount << 32) ^ (u64)c->h_job.L;
+    return job_shape_key(c->h_job.base, c->h_job.kcount, c->h_job.L);
 }
 
 // Starts the per-job tuner: the candidates are the geometries whose model cost
@@ -223,8 +240,11 @@ static void tune_start(rs_ctx *c)
         if (geom_model_cost(g, c->h_job.kcount, c->h_job.L) <= 2.0 * best) c->tune_cand[c->tune_ncand++] = g;
     c->geom = gb;
     c->tuning = (c->tune_ncand > 1);
-    for (const auto &t : c->tuned)
-        if (t.first == job_shape(c)) { c->geom = t.second; c->tuning = false; }
+    const int known = tuned_geom_get(c->device, job_shape(c));
+    if (known >= 0) {
+        c->geom = known;
+        c->tuning = false;
+    }
 }
 
 // Records one chunk's BSGS time; ends tuning once every candidate has timed at
@@ -243,7 +263,7 @@ static void tune_record(rs_ctx *c, int g, u32 primes, float ms)
         if (v < best) { best = v; c->geom = gi; }
     }
     c->tuning = false;
-    c->tuned.emplace_back(job_shape(c), c->geom);
+    tuned_geom_put(c->device, job_shape(c), c->geom);
 }
 
 extern "C" int rs_set_baby_steps(rs_ctx *c, uint32_t q)

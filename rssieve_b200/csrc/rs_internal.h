@@ -58,6 +58,14 @@ inline int geom_model_best(u32 kcount, u32 L)
         if (geom_model_cost(g, kcount, L) < geom_model_cost(best, kcount, L)) best = g;
     return best;
 }
+// Measured geometries per device and job shape (base, kcount, L), shared by the
+// single-job contexts and the batches of the process; -1 when none is recorded.
+inline u64 job_shape_key(u32 base, u32 kcount, u32 L)
+{
+    return ((u64)base << 40) ^ ((u64)kcount << 32) ^ (u64)L;
+}
+int tuned_geom_get(int device, u64 shape);
+void tuned_geom_put(int device, u64 shape, int geom);
 constexpr int BSGS_MAXPROBE = 64;
 constexpr int BSGS_SPEC_PROBE = 64;         // bucket walk bound while ord(s) is still unknown
 

@@ -179,3 +179,26 @@ def test_batch_config4_job_matches_single_job_path(rs, sieve):
         assert b.job_info(j)[1] == cnt["primes"]
     finally:
         b.close()
+
+
+def test_job_footprint_and_memory_reserve(rs, sieve):
+    """A job's footprint is its bitmap plus a 16-byte factor record per candidate
+    (and one spare); a reserve of a few footprints maps, and clones admitted
+    within it run as usual."""
+    job = W.small_job(60, kcount=10, base=2, nmin=1000, nmax=20000, keep=0.3, kmax=1 << 24)
+    seqs = W.seqs_of(job)
+    b = rs.Batch(0, max_jobs=4, range_slots=4)
+    try:
+        t = b.add(seqs, 3, 3)
+        fb = b.job_bytes(t)
+        assert fb == seqs.kcount * seqs.words_per_seq * 4 + (seqs.count() + 1) * 16
+        assert b.reserve(4 * fb)
+        j1 = b.add_clone(t, 3, 150_000, 2)
+        j2 = b.add_clone(t, 150_000, 300_000, 2)
+        assert b.job_bytes(j1) == b.job_bytes(j2) == fb
+        assert b.run(0)
+        sieve.load(seqs)
+        sieve.run(3, 300_000)
+        assert _terms(b.factors(j1)) | _terms(b.factors(j2)) == _terms(sieve.factors())
+    finally:
+        b.close()

@@ -128,3 +128,9 @@ def test_tuner_runs_candidates_and_matches_fixed_q(sieve, rs):
     assert cnt_auto["primes"] == cnt_fixed["primes"]
     assert set(zip(fa["seq"].tolist(), fa["n"].tolist())) == set(zip(ff["seq"].tolist(), ff["n"].tolist()))
     assert np.array_equal(bma, bmf)
+    # a batch job of the same shape takes the measured Q, not the cost model's
+    b = rs.Batch(0, max_jobs=1, range_slots=1)
+    try:
+        assert b.job_info(b.add(W.seqs_of(job), p0, p0))[0] == q_auto
+    finally:
+        b.close()
