@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--baby-steps", type=int, default=0, help="fix Q baby steps per prime (0: the per-job tuner)")
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the batched (configs 2, 3, 4) and served (config 5) forms")
+    ap.add_argument("--serve-rates", default="", help="extra arrival rates (units/s, comma-separated) to serve")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     return ap.parse_args()
 
@@ -229,8 +230,10 @@ def measure_served(rs, W, serve, seed=5, nunits=60, rate=8.0, width_log2=(22, 26
     units = [serve.Unit(k, fi, p0, p1, t) for k, (t, fi, p0, p1) in enumerate(raw)]
     srv = serve.Server(files, max_units=48, range_slots=64)
     try:
+        busy0 = srv.busy_s
         out = srv.run(units)
         st = serve.latency_stats(out)
+        st["gpu_busy"] = (srv.busy_s - busy0) / st["span_s"]
         ratios = []
         for u in out:
             v = serve.Unit(u.uid, u.file, u.p0, u.p1, 0.0)
@@ -241,7 +244,9 @@ def measure_served(rs, W, serve, seed=5, nunits=60, rate=8.0, width_log2=(22, 26
     st.update({"workload": "config5 shape scaled down: %d units over 16 files, Poisson %.0f units/s, widths 2^%d..2^%d, "
                            "starts 2^44..2^62" % (nunits, rate, width_log2[0], width_log2[1]),
                "latency_over_isolated_p50": float(np.percentile(ratios, 50)),
-               "latency_over_isolated_p99": float(np.percentile(ratios, 99))})
+               "latency_over_isolated_p99": float(np.percentile(ratios, 99)),
+               "latency_over_isolated_max": float(max(ratios)),
+               "policy": "%s, %.0f ms rounds" % (srv.policy, srv.round_s * 1e3)})
     return st
 
 
@@ -397,6 +402,9 @@ def main():
                  "batched_config4": measure_one_job_batched(torch, rs, W, W.config4(), (1 << 64) - (1 << 36), 30, 32,
                                                             "config4 job (b=5, 20 seqs, k even < 2^40, p near 2^64)"),
                  "served": measure_served(rs, W, serve)}
+        rates = [float(x) for x in args.serve_rates.split(",") if x] if args.serve_rates else []
+        if rates:
+            forms["served_sweep"] = [measure_served(rs, W, serve, rate=r) for r in rates]
 
     if rank == 0:
         line = {

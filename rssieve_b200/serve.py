@@ -5,13 +5,16 @@ and candidate bitmap).  Every file is held on the device once, as a resident
 batch template (rs_batch_add with an empty range); a unit is admitted as a
 device-side clone of its file's template with its own bitmap, so its result
 does not depend on which other units share the device.  Admission is by free
-batch slots and device memory: a unit that arrives while others are running
-joins at the next round boundary, spread over a few free range slots, runs
-alongside them (one BSGS launch per
-geometry group covers every admitted unit), and leaves when its range is done
--- its factors and bitmap are collected and its slots released for the next
-arrival.  Every round the units share a budget of work, shortest remaining
-first.  Latency is measured from arrival and from admission.
+batch slots and HBM footprint: the server maps a memory reserve for unit
+buffers once, at start, and admits a unit only while the footprints of the
+admitted units (bitmap plus a factor list with room for every candidate) fit
+in it, so no admission waits for new device memory.  A unit that arrives while
+others are running joins at the next round boundary, spread over a few free
+range slots, runs alongside them (one BSGS launch per geometry group covers
+every admitted unit), and leaves when its range is done -- its factors and
+bitmap are collected and its slots and memory released for the next arrival.
+Every round the units share a budget of work, shortest remaining first.
+Latency is measured from arrival and from admission.
 """
 import math
 import time
@@ -46,44 +49,76 @@ def cost_per_prime(q, kcount, L):
 class Server:
     """Continuous-batching sieve server over one device.
 
-    Each round, units are ordered by their estimated remaining work (primes
-    left times the model cost of one prime for their file) and given primes to
-    cover from a round budget -- shortest remaining first -- so that a short
-    unit arriving while long ones run finishes within a round or two.  The
-    budget is ROUND_S seconds of the measured throughput.  A unit spreads over
-    at most MAX_SPLIT range slots, enough to take a whole round's budget, so
-    that slots stay free for arrivals."""
+    Each round, units are put in priority order (earliest deadline first by
+    default, or least remaining work first; work is primes left times the model
+    cost of one prime for the unit's file) and given primes to cover from a
+    round budget of ROUND_S seconds of the measured throughput, so that a short
+    unit arriving while long ones run finishes within a round or two.  A unit
+    spreads over at most MAX_SPLIT range slots, enough to take a whole round's
+    budget, so that slots stay free for arrivals."""
 
     PRIMES_PER_SLOT_ROUND = 0.6 * 65536    # one range slot's round capacity
-    ROUND_S = 0.006                        # target round duration
+    ROUND_S = 0.004                        # target round duration
     MIN_ROUND_S = 0.0015                   # shortest round when a unit is about to finish
+    SLOWDOWN = 2.0                         # deadline: arrival + SLOWDOWN x estimated time alone
     MAX_SPLIT = 4                          # range slots per unit: a few absorb a round's budget,
                                            # the rest stay free for new arrivals
 
-    def __init__(self, files, device=0, max_units=48, range_slots=128, round_s=None, short_rounds=True):
+    MAX_RESERVE = 64 << 30                 # largest memory reserve for unit buffers (bytes)
+
+    def __init__(self, files, device=0, max_units=48, range_slots=128, round_s=None, short_rounds=False,
+                 reserve_bytes=None, policy="edf"):
         nf = len(files)
         self.round_s = round_s or self.ROUND_S
         self.short_rounds = short_rounds
+        if policy not in ("edf", "srpt"):
+            raise ValueError("policy is 'edf' or 'srpt'")
+        self.policy = policy
         self.batch = Batch(device, max_jobs=nf + max_units, range_slots=range_slots)
-        self.templates, self.cost = [], {}
+        self.templates, self.cost, self.footprint = [], {}, {}
         for seqs in files:
             t = self.batch.add(seqs, 3, 3)        # p0 == p1: resident template, never runs
             assert t is not None
             self.templates.append(t)
             self.cost[t] = cost_per_prime(self.batch.job_info(t)[0], seqs.kcount, seqs.nmax - seqs.nmin + 1)
+            self.footprint[t] = self.batch.job_bytes(t)
         self.max_units = max_units
+        # memory for max_units of the largest footprint, within MAX_RESERVE; halved until the device has it
+        want = reserve_bytes or min(max_units * max(self.footprint.values()), self.MAX_RESERVE)
+        while not self.batch.reserve(want):
+            want //= 2
+            if want < max(self.footprint.values()):
+                raise MemoryError("no device memory for one unit's buffers")
+        self.reserve = want
+        self.in_use = 0                           # footprint of the admitted units
         self.rate = None                          # cost units per second, measured
+        self.busy_s = 0.0                         # time spent in rounds, over all runs
 
     def close(self):
         self.batch.close()
 
+    def _work(self, u, width):
+        """Model cost of sieving `width` of unit u's p-range."""
+        return width / math.log(max(u.p0, 3)) * self.cost[self.templates[u.file]]
+
     def _budgets(self, active, remaining, given):
-        """Shortest remaining first: primes per unit for the next round (calls the
-        library only where a unit's budget changes)."""
+        """Primes per unit for the next round, in priority order, from a budget of
+        ROUND_S seconds of measured throughput (calls the library only where a
+        unit's budget changes).  'srpt': least remaining work first.  'edf':
+        earliest deadline first, a unit's deadline being its arrival plus
+        SLOWDOWN times its estimated time alone (its work at the measured rate,
+        plus a round) -- short units come first, and a long unit that has waited
+        overtakes them before its latency reaches SLOWDOWN times its own."""
         def left(slot):
-            u = active[slot]
-            return remaining[slot] / math.log(max(u.p0, 3)) * self.cost[self.templates[u.file]]
-        order = sorted(active, key=left)
+            return self._work(active[slot], remaining[slot])
+        if self.policy == "edf" and self.rate is not None:
+            def deadline(slot):
+                u = active[slot]
+                alone = self._work(u, u.p1 - u.p0) / self.rate + self.round_s
+                return u.arrival + self.SLOWDOWN * alone
+            order = sorted(active, key=deadline)
+        else:
+            order = sorted(active, key=left)
         budget = None if self.rate is None else self.rate * self.round_s
         if budget is not None and self.short_rounds and order:
             # a unit that finishes this round shares it with at most as much other work
@@ -121,6 +156,9 @@ class Server:
             # free range slots as finish it in about one round
             while queue and len(active) < self.max_units:
                 u = queue[0]
+                need = self.footprint[self.templates[u.file]]
+                if self.in_use + need > self.reserve:
+                    break
                 free = self.batch.free_slots()[1]
                 if free == 0:
                     break
@@ -130,6 +168,7 @@ class Server:
                 if slot is None:
                     break
                 u.admitted = clock() - t0
+                self.in_use += need
                 active[slot] = u
                 remaining[slot] = u.p1 - u.p0
                 primes_seen[slot] = 0
@@ -146,6 +185,7 @@ class Server:
             self.batch.run(1)                        # one round for every unit with a budget
             done, primes, rem = self.batch.poll()
             dt = clock() - r0
+            self.busy_s += dt
             work = sum(float(primes[s] - primes_seen[s]) * self.cost[self.templates[active[s].file]] for s in active)
             if trace is not None:
                 trace.append({"t": r0 - t0, "dt": dt, "rate": self.rate, "work": work, "queue": len(queue),
@@ -170,6 +210,7 @@ class Server:
                 if collect_bitmaps:
                     u.bitmap = self.batch.bitmap(slot)
                 self.batch.release(slot)
+                self.in_use -= self.footprint[self.templates[u.file]]
         return units
 
 
