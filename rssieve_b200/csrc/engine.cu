@@ -6,6 +6,7 @@
 // plumbing of simpleCL.c.  One CUDA stream per context; the host waits once
 // per segment for the prime count, then launches set-up and BSGS over chunks
 // of primes.  Device counters and the factor buffer accumulate across calls.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -51,6 +52,7 @@ struct rs_ctx {
     size_t bitmap_words = 0;
     FactorRec *d_factors = nullptr;
     u32 factor_cap = 0;
+    size_t bitmap_alloc = 0, factor_alloc = 0;   // capacities (words, records): buffers only grow
     u64 primes_total = 0;
     // BSGS geometry: forced (index into BSGS_GEOMS) or chosen per job by the tuner
     int geom_forced = -1;
@@ -82,6 +84,7 @@ static void free_job(rs_ctx *c)
     cudaFree(c->d_factors);
     c->d_bitmap = nullptr;
     c->d_factors = nullptr;
+    c->bitmap_alloc = c->factor_alloc = 0;
     c->job_loaded = false;
 }
 
@@ -313,17 +316,27 @@ extern "C" int rs_job_load(rs_ctx *c, const rs_seqs *s)
     int rc = rs_seqs_validate(s);
     if (rc) return rc;
     CU(cudaSetDevice(c->device));
-    free_job(c);
+    c->job_loaded = false;
     JobDev J;
     jobdev_from_seqs(s, &J);
     c->bitmap_words = (size_t)s->kcount * s->words_per_seq;
     uint64_t cand = rs_seqs_count(s);
     c->factor_cap = (u32)std::min<uint64_t>(cand + 1, 0xFFFFFFF0ull);
-    if (cudaMalloc(&c->d_bitmap, c->bitmap_words * 4) != cudaSuccess ||
-        cudaMalloc(&c->d_factors, (size_t)c->factor_cap * sizeof(FactorRec)) != cudaSuccess) {
+    // the buffers of an earlier job are reused when large enough: a fresh
+    // allocation synchronises the device and maps new memory, which costs more
+    // than the upload itself when jobs are loaded one after another
+    if (c->bitmap_words > c->bitmap_alloc || c->factor_cap > c->factor_alloc) {
+        const size_t bw = std::max(c->bitmap_words, c->bitmap_alloc);
+        const size_t fr = std::max((size_t)c->factor_cap, c->factor_alloc);
         free_job(c);
-        rs_set_error("cannot allocate the bitmap (%zu words) and factor buffer", c->bitmap_words);
-        return RS_ENOMEM;
+        if (cudaMalloc(&c->d_bitmap, bw * 4) != cudaSuccess ||
+            cudaMalloc(&c->d_factors, fr * sizeof(FactorRec)) != cudaSuccess) {
+            free_job(c);
+            rs_set_error("cannot allocate the bitmap (%zu words) and factor buffer", c->bitmap_words);
+            return RS_ENOMEM;
+        }
+        c->bitmap_alloc = bw;
+        c->factor_alloc = fr;
     }
     J.bitmap = c->d_bitmap;
     c->h_job = J;
