@@ -20,6 +20,7 @@ bounded sample of the same workload with every host thread.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -39,6 +40,26 @@ P_START = 1 << 50
 # to primes, so the per-launch figure is this times the primes one launch
 # processes.
 BSGS_DRAM_BYTES_PER_PRIME = 2132.9
+
+
+def reference_params(nmin, nmax):
+    """The reference's BSGS parameters for an n-range (cl_sieve.cpp:893-938): Q
+    doubles from 1024 while below both 4096 and ceil(sqrt(L)); M = ceil(L/Q) giant
+    steps for full-range sequences, MM = ceil(L/2Q) for single-parity ones."""
+    L = nmax - nmin + 1
+    target = math.ceil(math.sqrt(L))
+    q = 1024
+    while q < 4096 and q < target:
+        q <<= 1
+    return {"Q": q, "M": -(-L // q), "MM": -(-L // (2 * q))}
+
+
+def mulmod_rates(counters, seconds, peak_g):
+    """Giant-step products (one modular product each) and baby steps per second
+    over a whole run, and the giant rate as a fraction of the measured peak."""
+    g = counters["giant"] / seconds
+    return {"giant_products_per_s": g, "baby_steps_per_s": counters["baby"] / seconds,
+            "giant_frac_of_mulmod_peak": g / (peak_g * 1e9)}
 
 
 def parse():
@@ -131,7 +152,7 @@ def cpu_baseline(seed, target_s, job=None):
                 len(pl), threads, dt, st["mulmods"] / dt)}
 
 
-def measure_batched(torch, rs, W, seed=3, njobs=48, window_log2=24):
+def measure_batched(torch, rs, W, peak_g, seed=3, njobs=48, window_log2=24):
     """Config-3 sample: the same jobs and p-windows through the single-job path, job
     after job, and through one batch.  CUDA events on one side stream bracket the
     uploads (each job's bitmap and tables, from pageable host memory) and the
@@ -146,13 +167,17 @@ def measure_batched(torch, rs, W, seed=3, njobs=48, window_log2=24):
     sv = rs.Sieve(torch.cuda.current_device())
     sv.set_stream(st.cuda_stream)
     plain_terms, plain_primes, load_ms, run_ms = [], 0, 0.0, 0.0
+    plain_ctr = {"giant": 0, "baby": 0}
     torch.cuda.synchronize()
     for sq, (p0, p1) in zip(seqs, wins):
         e = [ev() for _ in range(3)]
         e[0].record(st)
         sv.load(sq)
         e[1].record(st)
-        plain_primes += sv.run(p0, p1)["primes"]
+        c = sv.run(p0, p1)
+        plain_primes += c["primes"]
+        for k in plain_ctr:
+            plain_ctr[k] += c[k]
         e[2].record(st)
         torch.cuda.synchronize()
         load_ms += e[0].elapsed_time(e[1])
@@ -175,6 +200,7 @@ def measure_batched(torch, rs, W, seed=3, njobs=48, window_log2=24):
     same = all(set(zip(f["seq"].tolist(), f["n"].tolist())) == t
                for f, t in zip((b.factors(j) for j in ids), plain_terms))
     qs = sorted(set(b.job_info(j)[0] for j in ids))
+    batch_ctr = b.counters()
     b.close()
     return {"workload": "config3 sample: %d jobs (1-100 seqs, b in {2,3,5,6,10}, n from 1e6, p from 2^44..2^60), "
                         "2^%d-wide p-window each" % (njobs, window_log2),
@@ -186,10 +212,12 @@ def measure_batched(torch, rs, W, seed=3, njobs=48, window_log2=24):
                              "batched_primes_per_s": batch_primes / ((b_load + b_run) / 1e3),
                              "batched_over_plain": (load_ms + run_ms) / (b_load + b_run),
                              "upload_ms": {"plain": load_ms, "batched": b_load}},
+            "mulmods": {"plain": mulmod_rates(plain_ctr, run_ms / 1e3, peak_g),
+                        "batched": mulmod_rates(batch_ctr, b_run / 1e3, peak_g)},
             "identical_eliminated_terms": bool(same and plain_primes == batch_primes), "baby_steps_used": qs}
 
 
-def measure_one_job_batched(torch, rs, W, job, p0, width_log2, nsplit, label):
+def measure_one_job_batched(torch, rs, W, peak_g, job, p0, width_log2, nsplit, label):
     """One job over one p-window through the single-job path and through the batch
     (a resident copy of the job cloned over nsplit range slots, at the Q the
     single-job tuner measured for the job's shape); CUDA events on one side stream
@@ -206,7 +234,8 @@ def measure_one_job_batched(torch, rs, W, job, p0, width_log2, nsplit, label):
     sv.load(seqs)
     torch.cuda.synchronize()
     ev[0].record(st)
-    plain_primes = sv.run(p0, p1)["primes"]
+    plain_ctr = sv.run(p0, p1)
+    plain_primes = plain_ctr["primes"]
     ev[1].record(st)
     torch.cuda.synchronize()
     f = sv.factors()
@@ -226,16 +255,19 @@ def measure_one_job_batched(torch, rs, W, job, p0, width_log2, nsplit, label):
     q, batch_primes, _ = b.job_info(j)
     same = (set(zip(f["seq"].tolist(), f["n"].tolist())) == plain_terms and batch_primes == plain_primes
             and np.array_equal(b.bitmap(j), plain_bm))
+    batch_ctr = b.counters()
     b.close()
     pms, bms = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
     return {"workload": "%s: one 2^%d-wide p-window from %s, batch over %d range slots" % (
                 label, width_log2, hex(p0), nsplit),
             "primes": int(batch_primes), "plain_primes_per_s": plain_primes / (pms / 1e3),
             "batched_primes_per_s": batch_primes / (bms / 1e3), "batched_over_plain": pms / bms,
+            "mulmods": {"plain": mulmod_rates(plain_ctr, pms / 1e3, peak_g),
+                        "batched": mulmod_rates(batch_ctr, bms / 1e3, peak_g)},
             "identical_eliminated_terms": bool(same), "baby_steps_used": q}
 
 
-def measure_served(rs, W, serve, seed=5, nunits=60, rate=8.0, width_log2=(22, 26)):
+def measure_served(rs, W, serve, peak_g, seed=5, nunits=60, rate=8.0, width_log2=(22, 26)):
     """Config-5 shape, scaled down: 16 config-2-style files, Poisson arrivals at `rate`
     units/s, unit widths 2^22..2^26 (the full workload's are 2^30..2^36); latency
     from arrival and from admission, and each unit's latency over its own run time
@@ -246,10 +278,13 @@ def measure_served(rs, W, serve, seed=5, nunits=60, rate=8.0, width_log2=(22, 26
     units = [serve.Unit(k, fi, p0, p1, t) for k, (t, fi, p0, p1) in enumerate(raw)]
     srv = serve.Server(files, max_units=48, range_slots=64)
     try:
-        busy0 = srv.busy_s
+        busy0, c0 = srv.busy_s, srv.batch.counters()
         out = srv.run(units)
+        c1 = srv.batch.counters()
         st = serve.latency_stats(out)
         st["gpu_busy"] = (srv.busy_s - busy0) / st["span_s"]
+        st["mulmods_while_busy"] = mulmod_rates({k: c1[k] - c0[k] for k in ("giant", "baby")},
+                                                srv.busy_s - busy0, peak_g)
         ratios = []
         for u in out:
             v = serve.Unit(u.uid, u.file, u.p0, u.p1, 0.0)
@@ -412,15 +447,25 @@ def main():
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         from rssieve_b200 import serve
-        forms = {"batched": measure_batched(torch, rs, W),
-                 "batched_config2": measure_one_job_batched(torch, rs, W, job, P_START + (1 << 37), 29, 32,
+        forms = {"batched": measure_batched(torch, rs, W, peak),
+                 "batched_config2": measure_one_job_batched(torch, rs, W, peak, job, P_START + (1 << 37), 29, 32,
                                                             "config2 job"),
-                 "batched_config4": measure_one_job_batched(torch, rs, W, W.config4(), (1 << 64) - (1 << 36), 30, 32,
+                 "batched_config4": measure_one_job_batched(torch, rs, W, peak, W.config4(), (1 << 64) - (1 << 36),
+                                                            30, 32,
                                                             "config4 job (b=5, 20 seqs, k even < 2^40, p near 2^64)"),
-                 "served": measure_served(rs, W, serve)}
+                 "served": measure_served(rs, W, serve, peak)}
         rates = [float(x) for x in args.serve_rates.split(",") if x] if args.serve_rates else []
         if rates:
-            forms["served_sweep"] = [measure_served(rs, W, serve, rate=r) for r in rates]
+            forms["served_sweep"] = [measure_served(rs, W, serve, peak, rate=r) for r in rates]
+
+    # work per prime against the reference's parameter rule on the same primes: its Q
+    # baby steps per searched prime, and the giant steps scaled by its M over ours
+    rp = reference_params(job["nmin"], job["nmax"])
+    searched = tot["full"] + tot["parity"]
+    m_ours = -(-(job["nmax"] - job["nmin"] + 1) // baby_q)
+    work_ours = tot["baby"] + tot["giant"]
+    work_ref = rp["Q"] * searched + tot["giant"] * rp["M"] / m_ours
+    rp["work_per_prime_est"] = work_ref / max(tot["primes"], 1)
 
     if rank == 0:
         line = {
@@ -447,7 +492,9 @@ def main():
                        "skipped": tot["skipped"], "factors": int(len(fac)), "dups": tot["dups"],
                        "candidates": tot["candidates"], "bsgs_ms_avg": bsgs_ms_avg,
                        "bsgs_share": bsgs_ms / max(dev_ms, 1e-9), "wall_s": wall,
-                       "mont_products_per_s": giant_all / (dev_ms_max / 1e3)},
+                       "mont_products_per_s": giant_all / (dev_ms_max / 1e3),
+                       "work_per_prime": work_ours / max(tot["primes"], 1), "reference_rule": rp,
+                       "work_ref_over_ours": work_ref / max(work_ours, 1)},
         }
         print(json.dumps(line), flush=True)
     sv.close()

@@ -138,9 +138,10 @@ class Server:
                 self.batch.set_budget(slot, n)
                 given[slot] = n
 
-    def run(self, units, clock=time.perf_counter, collect_bitmaps=False, trace=None):
+    def run(self, units, clock=time.perf_counter, collect_bitmaps=False, trace=None, sleep=time.sleep):
         """Serve the units (sorted by arrival time); returns them with timings filled.
-        trace: an optional list that receives one record per round."""
+        trace: an optional list that receives one record per round; clock and sleep
+        are the time source and the idle wait (seconds)."""
         pending = sorted(units, key=lambda u: u.arrival)
         queue, active = [], {}
         remaining, given = {}, {}
@@ -178,7 +179,7 @@ class Server:
                 if i < len(pending):                 # idle until the next arrival
                     wait = pending[i].arrival - (clock() - t0)
                     if wait > 0:
-                        time.sleep(wait)
+                        sleep(wait)
                 continue
             self._budgets(active, remaining, given)
             r0 = clock()
