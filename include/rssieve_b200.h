@@ -198,7 +198,9 @@ void rs_batch_destroy(rs_batch *b);
 int rs_batch_set_stream(rs_batch *b, void *stream);
 /* Adds a job with its p-range [p0, p1) (3 <= p0 < p1, or p0 == p1 for a
  * template, see rs_batch_add_clone); q fixes its baby-step
- * count (as rs_set_baby_steps) or 0 takes the cost model's choice.  The job's
+ * count (as rs_set_baby_steps).  With q = 0 the job takes the count that a
+ * context (rs_run_range) on the same device measured for a job of the same
+ * shape (base, sequence count, n-range), else the cost model's choice.  The job's
  * bitmap is copied to the device.  *job (may be NULL) receives its slot.
  * RS_EBUSY when no job or range slot is free. */
 int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t p1, uint32_t q, uint32_t *job);

@@ -386,7 +386,8 @@ class Batch:
         _check(lib().rs_batch_set_stream(self._b, C.c_void_p(stream_handle)), "rs_batch_set_stream")
 
     def add(self, seqs, p0, p1, q=0):
-        """Add a job over [p0, p1); returns its slot, or None when no slot is free."""
+        """Add a job over [p0, p1) (p0 == p1: a resident template); q fixes its baby steps,
+        0 takes a measured or modelled choice.  Returns its slot, or None when no slot is free."""
         j = C.c_uint32(0)
         rc = lib().rs_batch_add(self._b, seqs._p, p0, p1, q, C.byref(j))
         if rc == RS_EBUSY:
