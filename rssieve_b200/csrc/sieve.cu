@@ -134,29 +134,122 @@ __global__ void __launch_bounds__(SIEVE_TPB) k_sieve_batch(const BatchWin *__res
     sieve_block(w.base_odd, w.nodd, blockIdx.x, sp, nsp, cands + (size_t)r * ccap, ccap, ctrs + r * BR_CTRS, err);
 }
 
+// Strong probable prime to base a (a < n), n - 1 = d * 2^t with d odd.
+__device__ __forceinline__ bool sprp_base(u64 n, const Mont &M, u64 d, int t, u64 a)
+{
+    const u64 mone = n - M.one;           // Montgomery form of -1
+    u64 x = mpow(to_mont(a, M), d, M);
+    if (x == M.one || x == mone) return true;
+    for (int s = 1; s < t; ++s) {
+        x = mmul(x, x, n, M.q);
+        if (x == mone) return true;
+    }
+    return false;
+}
+
 // Deterministic primality below 2^64: the seven strong-probable-prime bases
 // of verify_factor.c:102.
 __device__ bool is_prime_mr(u64 n)
 {
     if (n < MR_BOUND) return true;        // sieve survivor below 65537^2
     const u32 bases[7] = {2u, 325u, 9375u, 28178u, 450775u, 9780504u, 1795265022u};
-    Mont M = mont_init(n);
+    const Mont M = mont_init(n);
     const u64 nm1 = n - 1;
     const int t = __ffsll((long long)nm1) - 1;
     const u64 d = nm1 >> t;
-    const u64 mone = n - M.one;           // Montgomery form of -1
-    for (int i = 0; i < 7; ++i) {
-        u64 a = bases[i];                 // every base is below n >= 65537^2
-        u64 x = mpow(to_mont(a, M), d, M);
-        if (x == M.one || x == mone) continue;
-        bool ok = false;
-        for (int s = 1; s < t; ++s) {
-            x = mmul(x, x, n, M.q);
-            if (x == mone) { ok = true; break; }
-        }
-        if (!ok) return false;
-    }
+    for (int i = 0; i < 7; ++i)           // every base is below n >= 65537^2
+        if (!sprp_base(n, M, d, t, bases[i])) return false;
     return true;
+}
+
+// floor(sqrt(n))^2 == n, by the bitwise integer square root.
+__device__ bool is_square(u64 n)
+{
+    u64 r = 0, bit = 1ull << 62, x = n;
+    while (bit > x) bit >>= 2;
+    while (bit) {
+        if (x >= r + bit) { x -= r + bit; r = (r >> 1) + bit; }
+        else r >>= 1;
+        bit >>= 2;
+    }
+    return r * r == n;
+}
+
+// x / 2 mod n for odd n and x in [0, n); also halves a Montgomery residue.
+__device__ __forceinline__ u64 mhalf(u64 x, u64 n)
+{
+    return (x & 1) ? (x >> 1) + (n >> 1) + 1 : x >> 1;
+}
+
+// Strong Lucas probable-prime test with Selfridge's parameters: D is the first
+// of 5, -7, 9, -11, ... with Jacobi (D/n) = -1, P = 1, Q = (1 - D)/4; with
+// n + 1 = d * 2^s (d odd), n passes if U_d = 0 or V_(d*2^r) = 0 for some r < s.
+// U, V and Q^k run in Montgomery form through the doubling formulas
+// U_2k = U_k V_k, V_2k = V_k^2 - 2Q^k and the step k -> k+1 (U' = (U + V)/2,
+// V' = (D U + V)/2).  Returns 1 (probable prime), 0 (composite), or -1 when no
+// D turned up within 64 candidates (the caller then decides otherwise).
+// n is odd, above 65537^2 and below 2^64 - 1.
+__device__ int lucas_strong(u64 n, const Mont &M)
+{
+    int D = 5;
+    for (int tries = 0;; ++tries) {
+        if (tries == 64) return -1;
+        const u32 a = (u32)(D < 0 ? -D : D);
+        int j = jacobi32((u32)(n % a), a);                 // (n/a), then reciprocity
+        if ((a & 3) == 3 && (n & 3) == 3) j = -j;
+        if (D < 0 && (n & 3) == 3) j = -j;                 // (-1/n)
+        if (j == -1) break;
+        if (j == 0) return 0;                              // gcd(a, n) > 1 with a < n
+        if (tries == 8 && is_square(n)) return 0;          // a square has no such D
+        D = (D > 0) ? -(D + 2) : (-D + 2);
+    }
+    const int Qi = (1 - D) / 4;
+    const u64 Qm = to_mont(Qi >= 0 ? (u64)Qi : n - (u64)(-Qi), M);
+    const u64 Dm = to_mont(D >= 0 ? (u64)D : n - (u64)(-D), M);
+    const int s = __ffsll((long long)(n + 1)) - 1;
+    const u64 d = (n + 1) >> s;
+    u64 U = M.one, V = M.one, Qk = Qm;                     // k = 1: U_1 = 1, V_1 = P = 1
+    for (int bit = 62 - __clzll(d); bit >= 0; --bit) {
+        const u64 U2 = mmul(U, V, n, M.q);
+        const u64 V2 = msub(mmul(V, V, n, M.q), madd(Qk, Qk, n), n);
+        const u64 Qk2 = mmul(Qk, Qk, n, M.q);
+        if ((d >> bit) & 1) {
+            U = mhalf(madd(U2, V2, n), n);
+            V = mhalf(madd(mmul(Dm, U2, n, M.q), V2, n), n);
+            Qk = mmul(Qk2, Qm, n, M.q);
+        } else {
+            U = U2;
+            V = V2;
+            Qk = Qk2;
+        }
+    }
+    if (U == 0) return 1;
+    for (int r = 0; r < s; ++r) {
+        if (V == 0) return 1;
+        if (r + 1 < s) {
+            V = msub(mmul(V, V, n, M.q), madd(Qk, Qk, n), n);
+            Qk = mmul(Qk, Qk, n, M.q);
+        }
+    }
+    return 0;
+}
+
+// Deterministic primality of a sieve survivor below 2^64 (Baillie-PSW): a
+// strong probable prime to base 2 that also passes the strong Lucas test.  No
+// composite below 2^64 passes both (the base-2 strong pseudoprimes below 2^64
+// have been enumerated and each fails the Lucas test).  About 3.5 Miller-Rabin
+// rounds of work per prime instead of the seven bases of is_prime_mr, which
+// remains the answer when no Lucas parameter is found.
+__device__ bool is_prime_bpsw(u64 n)
+{
+    if (n < MR_BOUND) return true;        // sieve survivor below 65537^2
+    if (n == ~0ull) return false;         // 2^64 - 1 = 3 * 5 * 17 * 257 * 641 * 65537 * 6700417
+    const Mont M = mont_init(n);
+    const u64 nm1 = n - 1;
+    const int t = __ffsll((long long)nm1) - 1;
+    if (!sprp_base(n, M, nm1 >> t, t, 2)) return false;
+    const int l = lucas_strong(n, M);
+    return (l >= 0) ? (l == 1) : is_prime_mr(n);
 }
 
 // Warp-stride Miller-Rabin over cands[0, min(*cand_ctr, cand_cap)) with ballot compaction into primes.
@@ -173,7 +266,7 @@ __device__ __forceinline__ void mr_list(const u64 *__restrict__ cands, const u32
         bool pr = false;
         if (idx < n) {
             v = cands[idx];
-            pr = is_prime_mr(v);
+            pr = is_prime_bpsw(v);
         }
         u32 mask = __ballot_sync(0xFFFFFFFFu, pr);
         if (!mask) continue;
@@ -206,7 +299,7 @@ __global__ void __launch_bounds__(256) k_mr_batch(const u64 *__restrict__ cands,
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const u32 r = prefix_find(prefix_c, nr, i);
         const u64 v = cands[(size_t)r * ccap + (i - prefix_c[r])];
-        if (!is_prime_mr(v)) continue;
+        if (!is_prime_bpsw(v)) continue;
         const u32 pos = atomicAdd(&ctrs[r * BR_CTRS + 1], 1u);
         if (pos < rcap) primes[(size_t)r * rcap + pos] = v;
         else atomicOr(err, ERR_PRIME_OVERFLOW);

@@ -134,3 +134,57 @@ def test_tuner_runs_candidates_and_matches_fixed_q(sieve, rs):
         assert b.job_info(b.add(W.seqs_of(job), p0, p0))[0] == q_auto
     finally:
         b.close()
+
+
+def _mr7(n):
+    """Deterministic 64-bit primality (seven strong bases), for building test inputs."""
+    if n < 2:
+        return False
+    for q in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+        if n % q == 0:
+            return n == q
+    return all(_sprp(n, a) for a in (2, 325, 9375, 28178, 450775, 9780504, 1795265022) if a % n)
+
+
+def _sprp(n, a):
+    d, t = n - 1, 0
+    while d % 2 == 0:
+        d, t = d // 2, t + 1
+    x = pow(a, d, n)
+    if x in (1, n - 1):
+        return True
+    for _ in range(t - 1):
+        x = x * x % n
+        if x == n - 1:
+            return True
+    return False
+
+
+def _base2_strong_pseudoprimes():
+    """Composites that pass the base-2 strong test and survive the sieve (no
+    factor below 65537): 2^59 - 1 = 179951 * 3203431780337, and products
+    p(2p - 1) of two primes near 2^33 and 2^63."""
+    out = [(1 << 59) - 1]
+    for start in (65537, (1 << 31) + 1):          # odd starts: p steps over odd numbers
+        p, found = start, 0
+        while found < 6:
+            p += 2
+            n = p * (2 * p - 1)
+            if _mr7(p) and _mr7(2 * p - 1) and _sprp(n, 2):
+                out.append(n)
+                found += 1
+    return out
+
+
+def test_base2_strong_pseudoprimes_are_rejected(sieve, oracle):
+    """The prime generator's test must not stop at base 2: base-2 strong
+    pseudoprimes that survive the sieve are composite, the window around
+    2^59 - 1 equals the oracle's primes."""
+    samples = _base2_strong_pseudoprimes()
+    assert len(samples) == 13
+    for n in samples:
+        assert _sprp(n, 2) and not _mr7(n)
+        assert len(sieve.primes(n, n + 1)) == 0, n
+    lo = (1 << 59) - 1 - 200_000
+    got = np.sort(sieve.primes(lo, lo + 400_000))
+    assert np.array_equal(got, oracle.primes(lo, lo + 400_000))
