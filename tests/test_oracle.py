@@ -142,3 +142,17 @@ def test_verify_and_sort_drops_composite_and_flags_false(oracle):
     kept, bad, cs = oracle.verify_and_sort(job, f)
     assert bad
     assert kept.tolist() == [(5, real, 0)]
+
+
+def test_bench_reference_rule_matches_oracle_restatement(oracle):
+    """bench.py's statement of the reference's Q/M rule (cl_sieve.cpp:893-938),
+    used to report work per prime against it, agrees with the oracle's own
+    restatement on every config's n-range and on the rule's edges."""
+    import bench
+    ranges = [(100000, 299999), (4000000, 9999999), (1000000, 2999999), (1000, 1000), (1000, 2047),
+              (1000, 1000 + 1024 * 1024), (1000, 1000 + 1024 * 1024 + 1), (10 ** 6, 10 ** 6 + 10 ** 7)]
+    for nmin, nmax in ranges:
+        got = bench.reference_params(nmin, nmax)
+        want = oracle.ref_params(nmin, nmax)
+        assert (got["Q"], got["M"], got["MM"]) == (want["Q"], want["m"], want["mm"]), (nmin, nmax)
+    assert bench.reference_params(4000000, 9999999) == {"Q": 4096, "M": 1465, "MM": 733}
