@@ -215,7 +215,7 @@ int rs_batch_add_clone(rs_batch *b, uint32_t src, uint64_t p0, uint64_t p1, uint
 /* Primes a job should cover in each following round, spread over its
  * unfinished ranges (each range at most about 39 000 per round); 0 pauses it.
  * Jobs start with full windows.  A serving loop sets these per round to order
- * work (e.g. shortest remaining first). */
+ * work (e.g. earliest deadline or shortest remaining first). */
 int rs_batch_set_budget(rs_batch *b, uint32_t job, uint64_t primes);
 /* Every job slot's state in one read: done (job finished; 0 for free slots),
  * primes tested and p-range left to sieve -- arrays of max_jobs entries, each

@@ -13,7 +13,7 @@ others are running joins at the next round boundary, spread over a few free
 range slots, runs alongside them (one BSGS launch per geometry group covers
 every admitted unit), and leaves when its range is done -- its factors and
 bitmap are collected and its slots and memory released for the next arrival.
-Every round the units share a budget of work, shortest remaining first.
+Every round the units share a budget of work, earliest deadline first.
 Latency is measured from arrival and from admission.
 """
 import math
