@@ -124,12 +124,17 @@ int rs_factors_finalize(const char *path, const rs_state *st);
 /* Checkpoint files; replace write_state/read_state, cl_sieve.cpp:185-319.
  * When every k < 2^31 the file is the reference's 488-byte workStatus layout
  * with its additive state_sum; otherwise a versioned layout with 64-bit k.
- * rs_state_read validates the checksum and the job fields and fails with
- * RS_ESTATE otherwise. */
+ * rs_state_read validates the job fields, the p-range and the checksum and
+ * fails with RS_ESTATE otherwise: st is in/out, and on entry st->pmin and
+ * st->pmax must hold the run's p-range (read_state compares them first,
+ * cl_sieve.cpp:236-242). */
 int rs_state_write(const char *path, const rs_state *st, const rs_seqs *s);
 int rs_state_read(const char *path, rs_state *st, const rs_seqs *s);
-/* Both A/B files: newest valid one wins (cl_sieve.cpp:288-318).  Returns 1 and
- * fills st and which (0 = A, 1 = B) when a valid state exists, 0 when none. */
+/* Both A/B files: newest valid one wins (cl_sieve.cpp:288-318).  A file for
+ * another p-range is invalid before the two are compared, so a stale file of
+ * a different run never shadows a good one.  st->pmin/st->pmax are the run's
+ * range on entry.  Returns 1 and fills st and which (0 = A, 1 = B) when a
+ * valid state exists, 0 when none. */
 int rs_state_resume(const char *path_a, const char *path_b, rs_state *st, const rs_seqs *s, int *which);
 
 /* ---------------- device ---------------- */
@@ -156,6 +161,15 @@ int rs_device_count(void);
 int rs_set_baby_steps(rs_ctx *ctx, uint32_t q);
 /* The Q in use; *tuning (may be NULL) is 1 while candidates are being timed. */
 int rs_get_baby_steps(rs_ctx *ctx, uint32_t *q, int *tuning);
+/* Bounded device waits.  Each CTA of the BSGS kernel waits for the next prime's
+ * record copy for at most `tries` rounds of mbarrier try_wait (0: the default,
+ * 2^24 rounds); when a wait runs out, the CTA lets the copy land, stops, and
+ * rs_run_range returns RS_EDEVICE with error flag 0x10, leaving the context
+ * usable.  test_stall = 1 sends each CTA's first wait to a barrier that
+ * nothing completes, so the bound always runs out: it exists to test that path
+ * (the reference's host polls its queue without bound, cl_sieve.cpp:331-379;
+ * there is no counterpart).  Takes effect at the next rs_run_range. */
+int rs_set_wait_limit(rs_ctx *ctx, uint32_t tries, int test_stall);
 /* Upload a job: sequences, n-range and bitmap (cl_sieve.cpp:1115-1120,1266). */
 int rs_job_load(rs_ctx *ctx, const rs_seqs *s);
 /* Sieve every prime in [p0,p1) (3 <= p0 < p1 <= 2^64-1): one pass of the

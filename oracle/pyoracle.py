@@ -42,9 +42,14 @@ _lib = None
 _ref = None
 
 
-def build():
-    """Compile the oracle (and the reference kernels when the reference tree exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+def build(refdir=None):
+    """Compile the oracle, and the reference kernels when refdir (default: the
+    RSSIEVE_REFERENCE_DIR environment variable) names the reference checkout."""
+    refdir = refdir or os.environ.get("RSSIEVE_REFERENCE_DIR", "")
+    cmd = ["make", "-s", "-C", HERE]
+    if refdir:
+        cmd.append("REFDIR=" + os.path.abspath(refdir))
+    subprocess.run(cmd, check=True)
 
 
 def lib():
@@ -74,6 +79,8 @@ def lib():
         L.or_setup.argtypes = [C.POINTER(_Job), u32, p64, C.c_size_t, p64, C.c_void_p]
         L.or_verify_and_sort.restype = C.c_size_t
         L.or_verify_and_sort.argtypes = [C.POINTER(_Job), C.c_void_p, C.c_size_t, C.POINTER(C.c_int), p64]
+        L.or_plant.restype = C.c_int
+        L.or_plant.argtypes = [u64, u32, i32, u32, u32, u64, C.c_int, p64, C.POINTER(u32)]
         L.or_m_mul.restype = u64
         L.or_m_mul.argtypes = [u64, u64, u64, u64]
         L.or_invert.restype = u64
@@ -175,6 +182,14 @@ def bsgs(job, plist, nthreads=1, cap=1 << 22):
     assert n <= cap, "oracle factor buffer overflow"
     stats = {f: int(getattr(st, f)) for f, _ in _Stats._fields_}
     return out[:n].copy(), stats, bm
+
+
+def plant(p, base, c, n_lo, n_hi, kmax, parity=-1):
+    """(k, n) with p | k*base^n+c, n in [n_lo, n_hi), k < kmax of the given
+    parity (0 even, 1 odd, -1 any), the first such n; None when none exists."""
+    k, n = C.c_uint64(0), C.c_uint32(0)
+    ok = lib().or_plant(p, base, c, n_lo, n_hi, kmax, parity, C.byref(k), C.byref(n))
+    return (int(k.value), int(n.value)) if ok else None
 
 
 def ref_params(nmin, nmax):

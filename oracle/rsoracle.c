@@ -676,3 +676,35 @@ size_t or_verify_and_sort(const or_job *job, or_factor *f, size_t nf, int *false
     if (checksum) *checksum = cs;
     return kept;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Test-input helper (not a restatement): planted factors                   */
+/* ------------------------------------------------------------------------ */
+
+/* Finds a term k*b^n+c that the prime p divides, with n in [n_lo, n_hi) and
+ * k < kmax of the wanted parity (par: 0 even, 1 odd, -1 either).  Walks n up
+ * from n_lo with t_n = -c*b^-n mod p, so k = t_n is the only k < p with
+ * p | k*b^n+c; returns 1 with the first hit, 0 when none exists in the range.
+ * Lets parity tests place known factors in the p-windows of the benchmark
+ * configurations, where random jobs have almost none. */
+int or_plant(uint64_t p, uint32_t b, int32_t c, uint32_t n_lo, uint32_t n_hi, uint64_t kmax, int par,
+             uint64_t *k_out, uint32_t *n_out)
+{
+    if (p < 3 || !(p & 1) || b % p == 0 || n_lo >= n_hi) return 0;
+    const uint64_t q = or_invert(p), one = (0 - p) % p, r2 = r2_of(p, q, one);
+    const uint64_t binv = inv_euclid(b % p, p);
+    const uint64_t mbinv = or_m_mul(binv, r2, p, q);
+    /* t = -c * binv^n_lo, in Montgomery form */
+    uint64_t t = or_powmod(mbinv, n_lo, p, q, one);
+    if (c == 1) t = t ? p - t : 0;
+    for (uint64_t n = n_lo; n < n_hi; ++n) {
+        const uint64_t k = or_m_mul(t, 1, p, q);
+        if (k && k < kmax && (par < 0 || (int)(k & 1) == par)) {
+            *k_out = k;
+            *n_out = (uint32_t)n;
+            return 1;
+        }
+        t = or_m_mul(t, mbinv, p, q);
+    }
+    return 0;
+}

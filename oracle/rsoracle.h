@@ -100,6 +100,13 @@ size_t or_bsgs(or_job *job, const uint64_t *primes, size_t np, int nthreads,
  * number kept (compacted in place).  *false_factor set if any verify failed. */
 size_t or_verify_and_sort(const or_job *job, or_factor *f, size_t nf, int *false_factor, uint64_t *checksum);
 
+/* ---- test-input helper (not a restatement) ----
+ * First n in [n_lo, n_hi) whose k = -c*b^-n mod p is below kmax with parity
+ * par (0 even, 1 odd, -1 any): then p | k*b^n+c.  Returns 1 and fills
+ * *k_out, *n_out, or 0 when there is none. */
+int or_plant(uint64_t p, uint32_t b, int32_t c, uint32_t n_lo, uint32_t n_hi, uint64_t kmax, int par,
+             uint64_t *k_out, uint32_t *n_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -51,7 +51,7 @@ EXPORTS = (
     "rs_state_resume", "rs_ctx_create", "rs_ctx_destroy", "rs_ctx_set_stream", "rs_device_count",
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
     "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_primes_generate_noalloc",
-    "rs_set_baby_steps", "rs_get_baby_steps",
+    "rs_set_baby_steps", "rs_get_baby_steps", "rs_set_wait_limit",
     "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone",
     "rs_batch_free_slots", "rs_batch_job_bytes", "rs_batch_reserve", "rs_batch_release", "rs_batch_set_budget",
     "rs_batch_poll", "rs_batch_run",
@@ -124,6 +124,7 @@ def lib():
         "rs_batch_job_info": (C.c_int, [vp, u32, C.POINTER(u32), C.POINTER(u64), C.POINTER(C.c_int)]),
         "rs_batch_counters": (C.c_int, [vp, C.POINTER(_Counters)]),
         "rs_get_baby_steps": (C.c_int, [vp, C.POINTER(u32), C.POINTER(C.c_int)]),
+        "rs_set_wait_limit": (C.c_int, [vp, u32, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -235,16 +236,18 @@ class State:
         _check(lib().rs_state_write(os.fsencode(path), C.byref(self.st), seqs._p), "rs_state_write")
 
     @classmethod
-    def read(cls, path, seqs):
-        s = cls()
+    def read(cls, path, seqs, pmin, pmax):
+        """The state in path, which must belong to seqs and to the p-range [pmin, pmax)."""
+        s = cls(pmin=pmin, pmax=pmax)
         rc = lib().rs_state_read(os.fsencode(path), C.byref(s.st), seqs._p)
         if rc != RS_OK:
             raise RSError(rc, "rs_state_read")
         return s
 
     @classmethod
-    def resume(cls, path_a, path_b, seqs):
-        s = cls()
+    def resume(cls, path_a, path_b, seqs, pmin, pmax):
+        """The newer valid one of two A/B state files of seqs over [pmin, pmax)."""
+        s = cls(pmin=pmin, pmax=pmax)
         which = C.c_int(-1)
         r = lib().rs_state_resume(os.fsencode(path_a), os.fsencode(path_b), C.byref(s.st), seqs._p, C.byref(which))
         return (s, which.value) if r == 1 else (None, -1)
@@ -346,6 +349,11 @@ class Sieve:
         q, t = C.c_uint32(0), C.c_int(0)
         _check(lib().rs_get_baby_steps(self._c, C.byref(q), C.byref(t)), "rs_get_baby_steps")
         return q.value, bool(t.value)
+
+    def set_wait_limit(self, tries=0, test_stall=False):
+        """Bound on the BSGS kernel's record-copy waits (0: default); test_stall
+        makes every CTA's first wait run out, to exercise the error path."""
+        _check(lib().rs_set_wait_limit(self._c, tries, 1 if test_stall else 0), "rs_set_wait_limit")
 
     def mulmod_peak(self):
         """10^9 Montgomery products/s of independent chains on this device."""

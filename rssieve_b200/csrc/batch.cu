@@ -348,6 +348,7 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
     if (cudaMallocFromPoolAsync((void **)&J.d_bitmap, J.bitmap_words * 4, b->pool, b->stream) != cudaSuccess ||
         cudaMallocFromPoolAsync((void **)&J.d_factors, (size_t)fcap * sizeof(FactorRec), b->pool, b->stream) !=
             cudaSuccess) {
+        cudaGetLastError();              // the failed pool allocation must not surface at the next round
         if (J.d_bitmap) cudaFreeAsync(J.d_bitmap, b->stream);
         if (J.d_factors) cudaFreeAsync(J.d_factors, b->stream);
         J = BJob();

@@ -168,7 +168,7 @@ struct RecBuf {
 };
 static_assert(sizeof(RecBuf) % 16 == 0, "bulk copies move 16-byte units");
 
-constexpr u32 WAIT_BOUND = 1u << 24;   // try_wait rounds before a copy is declared lost
+constexpr u32 WAIT_BOUND = 1u << 24;   // default try_wait rounds before a copy is declared lost
 
 // ---- per-CTA state in shared memory, read by the out-of-line rare paths ----
 // The hot loops stay small (and in the instruction cache) because matches,
@@ -406,8 +406,10 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
     u64 *s_start = Smem<TPB, NB>::start();
     u64 *s_Z = Smem<TPB, NB>::zs();
     RecBuf *rec = Smem<TPB, NB>::rec();                           // two staging buffers
-    __shared__ __align__(8) u64 s_bar[2];
+    __shared__ __align__(8) u64 s_bar[3];                        // [2]: never completed (failure test)
     __shared__ u32 s_idx[2], s_order, s_spill, s_abort;
+    const u32 wait_bound = a.wait_bound ? a.wait_bound : WAIT_BOUND;
+    u32 pend_buf = 0, pend_par = 0;                               // the copy waited for when aborting
 
     const u32 tid = threadIdx.x;
     auto fetch = [&](u32 buf, u32 idx) {                          // thread 0 only
@@ -422,6 +424,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
+        mbar_init(&s_bar[2], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_args = a;
         s_abort = 0;
@@ -438,11 +441,18 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         const u32 buf = it & 1;
         const u32 idx = s_idx[buf];
         if (idx == NONE) break;
-        // this prime's record was fetched one prime ago; the wait is bounded
+        // this prime's record was fetched one prime ago; the wait is bounded.
+        // A failure test sends the first wait to s_bar[2], which no copy or
+        // arrival ever completes, so the bound runs out.
+        pend_buf = buf;
+        pend_par = (it >> 1) & 1;
         {
+            const bool dead = (a.test_stall != 0) && (it == 0);
+            u64 *bar = dead ? &s_bar[2] : &s_bar[buf];
+            const u32 par = dead ? 0u : pend_par;
             u32 n = 0;
-            while (!mbar_try_wait(&s_bar[buf], (it >> 1) & 1)) {
-                if (++n > WAIT_BOUND) { atomicOr(&s_abort, 1u); break; }
+            while (!mbar_try_wait(bar, par)) {
+                if (++n > wait_bound) { atomicOr(&s_abort, 1u); break; }
             }
         }
         const RecBuf &R = rec[buf];
@@ -577,13 +587,14 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         atomicAdd(&a.stats[ST_FACTORS], s_facs);
         atomicAdd(&a.stats[ST_HITS], s_dups + s_facs);
     }
-    if (s_abort) {
-        // a record copy never completed: report, then give copies in flight a bounded chance to land
-        if (tid == 0) atomicOr(a.err, ERR_TMA_TIMEOUT);
-        for (int b = 0; b < 2; ++b) {
-            u32 n = 0;
-            while (n < WAIT_BOUND && !mbar_try_wait(&s_bar[b], 0) && !mbar_try_wait(&s_bar[b], 1)) ++n;
-        }
+    if (s_abort && tid == 0) {
+        // A record wait gave up.  The CTA stopped before fetching another record,
+        // so the only copy that can still be in flight is the one waited for:
+        // report, then let it land (bounded by the default) before the CTA's
+        // shared memory is released.
+        atomicOr(a.err, ERR_TMA_TIMEOUT);
+        u32 n = 0;
+        while (n < WAIT_BOUND && !mbar_try_wait(&s_bar[pend_buf], pend_par)) ++n;
     }
 }
 

@@ -159,7 +159,7 @@ int main(int argc, char **argv)
            seqs->nmax);
     bool write_a_next = true;
     int which = 0;
-    if (rs_state_resume(STATE_A, STATE_B, &st, seqs, &which) == 1 && st.pmin == pmin && st.pmax == pmax) {
+    if (rs_state_resume(STATE_A, STATE_B, &st, seqs, &which) == 1) {
         write_a_next = (which == 1);
         printf("Resuming from checkpoint in %s\nCurrent p: %" PRIu64 "\n", which ? STATE_B : STATE_A, st.p);
         fprintf(stderr, "Resuming from checkpoint, current p: %" PRIu64 "\n", st.p);

@@ -63,6 +63,9 @@ struct rs_ctx {
     double tune_ms[NGEOM];
     u64 tune_primes[NGEOM];
     std::vector<int> chunk_geom;
+    // bounded device waits (rs_set_wait_limit)
+    u32 wait_bound = 0;
+    u32 test_stall = 0;
     // timing of the last rs_run_range
     std::vector<cudaEvent_t> ev;
     double last_bsgs_ms = 0, last_total_ms = 0;
@@ -281,6 +284,14 @@ extern "C" int rs_set_baby_steps(rs_ctx *c, uint32_t q)
     return RS_OK;
 }
 
+extern "C" int rs_set_wait_limit(rs_ctx *c, uint32_t tries, int test_stall)
+{
+    if (!c || test_stall < 0 || test_stall > 1) return RS_EARG;
+    c->wait_bound = tries;
+    c->test_stall = (u32)test_stall;
+    return RS_OK;
+}
+
 extern "C" int rs_get_baby_steps(rs_ctx *c, uint32_t *q, int *tuning)
 {
     if (!c || !q) return RS_EARG;
@@ -473,6 +484,8 @@ extern "C" int rs_run_range(rs_ctx *c, uint64_t p0, uint64_t p1, rs_counters *de
     a.factor_cap = c->factor_cap;
     a.stats = c->d_stats;
     a.err = c->d_err;
+    a.wait_bound = c->wait_bound;
+    a.test_stall = c->test_stall;
     u64 p = p0;
     u64 width = segment_width(c, p);
     u64 seg_primes = 0;

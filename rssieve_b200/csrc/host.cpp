@@ -478,9 +478,14 @@ extern "C" int rs_state_write(const char *path, const rs_state *st, const rs_seq
     return RS_OK;
 }
 
+// st is in/out: on entry st->pmin and st->pmax are the run's p-range, and a
+// file written for another range is rejected like one for another job (the
+// reference's read_state compares base, pmin, pmax, nmin, nmax and kcount
+// before it looks at the checksum, cl_sieve.cpp:236-242,266-272).
 extern "C" int rs_state_read(const char *path, rs_state *st, const rs_seqs *s)
 {
     if (!path || !st || !s) return RS_EARG;
+    const uint64_t want_pmin = st->pmin, want_pmax = st->pmax;
     std::string data;
     FILE *f = fopen(path, "rb");
     if (!f) { rs_set_error("no checkpoint %s", path); return RS_EIO; }
@@ -495,7 +500,8 @@ extern "C" int rs_state_read(const char *path, rs_state *st, const rs_seqs *s)
     if (data.size() >= sizeof(WorkStatusV2) && memcmp(data.data(), kMagicV2, 8) == 0) {
         WorkStatusV2 w;
         memcpy(&w, data.data(), sizeof w);
-        if (w.base != s->base || w.nmin != s->nmin || w.nmax != s->nmax || w.kcount != (int32_t)s->kcount) {
+        if (w.base != s->base || w.pmin != want_pmin || w.pmax != want_pmax || w.nmin != s->nmin ||
+            w.nmax != s->nmax || w.kcount != (int32_t)s->kcount) {
             rs_set_error("Invalid checkpoint file %s", path);
             return RS_ESTATE;
         }
@@ -511,7 +517,8 @@ extern "C" int rs_state_read(const char *path, rs_state *st, const rs_seqs *s)
     if (data.size() < sizeof(WorkStatusV1)) { rs_set_error("Cannot parse %s", path); return RS_ESTATE; }
     WorkStatusV1 w;
     memcpy(&w, data.data(), sizeof w);
-    if (w.base != s->base || w.nmin != s->nmin || w.nmax != s->nmax || w.kcount != (int32_t)s->kcount) {
+    if (w.base != s->base || w.pmin != want_pmin || w.pmax != want_pmax || w.nmin != s->nmin || w.nmax != s->nmax ||
+        w.kcount != (int32_t)s->kcount) {
         rs_set_error("Invalid checkpoint file %s", path);
         return RS_ESTATE;
     }
@@ -528,7 +535,8 @@ extern "C" int rs_state_read(const char *path, rs_state *st, const rs_seqs *s)
 
 extern "C" int rs_state_resume(const char *path_a, const char *path_b, rs_state *st, const rs_seqs *s, int *which)
 {
-    rs_state a, b;
+    if (!st || !s) return RS_EARG;
+    rs_state a = *st, b = *st;             // both carry the run's pmin/pmax into rs_state_read
     bool ga = rs_state_read(path_a, &a, s) == RS_OK;
     bool gb = rs_state_read(path_b, &b, s) == RS_OK;
     if (ga && gb) {

@@ -12,10 +12,15 @@
 // most 2^21 odd values, which is exactly the survivor capacity, so the
 // survivor buffer can never overflow.  Wider ranges are rejected with RS_EARG.
 //
-// Set-up: the first call on a device (the device current on the calling
-// thread) looks up the scratch address with cudaGetSymbolAddress, fills the
+// Set-up: the first call in a CUDA context (the primary context of the device
+// current on the calling thread, or the driver-API context made current)
+// looks up the scratch address with cudaGetSymbolAddress, fills the
 // sieving-prime table with a one-CTA kernel on the caller's stream and waits
-// for that stream.  Later calls on the device only enqueue work and return.
+// for that stream.  Later calls in that context only enqueue work and return;
+// they still query the symbol address and the context's unique ID, so a
+// context created anew (after cudaDeviceReset, whose new context holds a
+// zeroed copy of the array) is set up again rather than trusted.  The first
+// call in a context should therefore come before any stream capture.
 //
 // What starts at zero: every call resets the survivor counter, the error word
 // and the caller's count word with cudaMemsetAsync on the caller's stream
@@ -45,13 +50,45 @@ static_assert(RS_NOALLOC_MAX_WIDTH / 2 == NA_CAND_CAP, "survivor capacity must c
 // are multiples of 256 bytes).
 static __device__ __align__(256) u64 g_na_scratch[NA_WORDS];
 
-constexpr int NA_MAX_DEVICES = 64;
-struct DevState {
+// Contexts set up so far, by the driver's unique context ID (never reused in
+// a process).  A context beyond the table's capacity replaces the oldest entry.
+constexpr int NA_MAX_CTX = 64;
+struct CtxState {
+    unsigned long long ctx_id = 0;    // 0: unused
     u64 *scratch = nullptr;
     int sms = 0;
 };
 std::mutex g_na_mu;
-DevState g_na_dev[NA_MAX_DEVICES];
+CtxState g_na_ctx[NA_MAX_CTX];
+int g_na_next = 0;
+
+// The unique ID of the calling thread's current context, through the driver
+// entry points the runtime exposes (no link against the driver library).
+typedef int (*CtxGetCurrentFn)(void **);
+typedef int (*CtxGetIdFn)(void *, unsigned long long *);
+int current_ctx_id(unsigned long long *id)
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void *f1 = nullptr, *f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+            rs_set_error("the CUDA driver does not provide cuCtxGetCurrent/cuCtxGetId");
+            return RS_ECUDA;
+        }
+        get_current = (CtxGetCurrentFn)f1;
+        get_id = (CtxGetIdFn)f2;
+    }
+    void *ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx || get_id(ctx, id) != 0) {
+        rs_set_error("no current CUDA context");
+        return RS_ECUDA;
+    }
+    return RS_OK;
+}
 
 // Odd primes below 2^16 in ascending order: one CTA sieves the 2^15 odd
 // values 2i+1 in shared memory and compacts them with a block-wide scan.
@@ -106,17 +143,10 @@ __global__ void __launch_bounds__(1024) k_na_small_primes(u32 *__restrict__ sp, 
         }                                                                                     \
     } while (0)
 
-// Once per device, with that device current: scratch address, SM count and
-// the sieving-prime table.  Waits for the caller's stream.
-int na_setup(int dev, cudaStream_t st, DevState *out)
+// Once per context, with it current: SM count and the sieving-prime table in
+// the scratch at ptr.  Waits for the caller's stream.
+int na_setup(int dev, void *ptr, cudaStream_t st, CtxState *out)
 {
-    void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_na_scratch);
-    if (e != cudaSuccess || !ptr) {
-        rs_set_error("cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev,
-                     cudaGetErrorString(e));
-        return RS_ECUDA;
-    }
     int sms = 0;
     NA_CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     u64 *scr = (u64 *)ptr;
@@ -163,19 +193,37 @@ extern "C" int rs_primes_generate_noalloc(uint64_t p0, uint64_t p1, uint64_t *d_
     }
     int dev = -1;
     NA_CU(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= NA_MAX_DEVICES) {
-        rs_set_error("device %d is beyond the %d devices this entry point tracks", dev, NA_MAX_DEVICES);
-        return RS_EARG;
+    // the address in this context (this also makes the runtime's context current)
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_na_scratch);
+    if (e != cudaSuccess || !ptr) {
+        rs_set_error("cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev,
+                     cudaGetErrorString(e));
+        return RS_ECUDA;
     }
+    unsigned long long cid = 0;
+    int rc = current_ctx_id(&cid);
+    if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    DevState ds;
+    CtxState ds;
     {
         std::lock_guard<std::mutex> lk(g_na_mu);
-        if (!g_na_dev[dev].scratch) {
-            int rc = na_setup(dev, st, &g_na_dev[dev]);
+        int slot = -1;
+        for (int i = 0; i < NA_MAX_CTX; ++i)
+            if (g_na_ctx[i].ctx_id == cid) slot = i;
+        if (slot < 0 || g_na_ctx[slot].scratch != (u64 *)ptr) {
+            if (slot < 0) {
+                slot = g_na_next;
+                g_na_next = (g_na_next + 1) % NA_MAX_CTX;
+            }
+            g_na_ctx[slot] = CtxState();
+            CtxState fresh;
+            rc = na_setup(dev, ptr, st, &fresh);
             if (rc) return rc;
+            fresh.ctx_id = cid;
+            g_na_ctx[slot] = fresh;
         }
-        ds = g_na_dev[dev];
+        ds = g_na_ctx[slot];
     }
     u64 *cands = ds.scratch;
     u32 *sp = (u32 *)(ds.scratch + NA_CAND_CAP);

@@ -80,6 +80,7 @@ constexpr u32 ERR_CAND_OVERFLOW = 2u;
 constexpr u32 ERR_HASH_OVERFLOW = 4u;       // a bucket chain exceeded BSGS_MAXPROBE
 constexpr u32 ERR_FACTOR_OVERFLOW = 8u;     // factor buffer full (cannot happen: sized to the bitmap)
 constexpr u32 ERR_TMA_TIMEOUT = 16u;        // a bulk copy did not complete within the wait bound
+constexpr u32 ERR_SIEVE_TABLE = 32u;        // the sieving-prime table is missing (does not start with 3)
 
 // statistics counters (u64)
 enum Stat {
@@ -145,6 +146,8 @@ struct BsgsArgs {
     u32 factor_cap;
     u64 *stats;
     u32 *err;
+    u32 wait_bound;      // try_wait rounds before a record copy counts as lost (0: WAIT_BOUND)
+    u32 test_stall;      // 1: each CTA's first record wait is on a barrier that nothing completes
 };
 
 // ---- batches: many jobs, each with one or more p-ranges, advanced in rounds ----

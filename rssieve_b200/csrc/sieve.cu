@@ -7,9 +7,10 @@
 // Eratosthenes sieve over 2^17 odd numbers in shared memory with every odd
 // prime below 2^16, compacts the survivors with warp ballots/popc, and a
 // second kernel proves the survivors at or above 65537^2 prime with the
-// 7-base strong-probable-prime test that verify_factor.c:100-128 uses
-// (deterministic below 2^64).  Survivors below 65537^2 are prime already.
-// The result is the exact set of odd primes in [lo, hi).
+// Baillie-PSW test (a base-2 strong probable-prime test, then a strong Lucas
+// test; deterministic below 2^64, see is_prime_bpsw).  Survivors below
+// 65537^2 are prime already.  The result is the exact set of odd primes in
+// [lo, hi).
 #include "mont.cuh"
 #include "rs_internal.h"
 
@@ -36,6 +37,12 @@ __device__ __forceinline__ void sieve_block(u64 base_odd, u64 nodd, u32 blk, con
     const u32 tid = threadIdx.x;
     const u64 i0 = (u64)blk * BITS;
     if (i0 >= nodd) return;
+    // the table must start with 3: an empty or zeroed table would make the
+    // one-prime-per-thread marking loop below step by 0 forever
+    if (nsp == 0 || sp[0] != 3u) {
+        if (tid == 0) atomicOr(err, ERR_SIEVE_TABLE);
+        return;
+    }
     const u32 nbits = (u32)min((u64)BITS, nodd - i0);
     const u64 bb = base_odd + 2 * i0;                   // value of bit 0 (odd)
     const u64 vlast = bb + 2 * (u64)(nbits - 1);
@@ -235,11 +242,15 @@ __device__ int lucas_strong(u64 n, const Mont &M)
 }
 
 // Deterministic primality of a sieve survivor below 2^64 (Baillie-PSW): a
-// strong probable prime to base 2 that also passes the strong Lucas test.  No
-// composite below 2^64 passes both (the base-2 strong pseudoprimes below 2^64
-// have been enumerated and each fails the Lucas test).  About 3.5 Miller-Rabin
-// rounds of work per prime instead of the seven bases of is_prime_mr, which
-// remains the answer when no Lucas parameter is found.
+// strong probable prime to base 2 that also passes the strong Lucas test with
+// Selfridge's parameters.  No composite below 2^64 passes both: J. Feitsma and
+// W. Galway enumerated every base-2 Fermat pseudoprime below 2^64 (published
+// 2009-2010, about 118.9 million numbers), and J. Gilchrist checked that none of
+// them is a strong Lucas probable prime with these parameters, i.e. there is no
+// Baillie-PSW pseudoprime below 2^64 (reported 2009, on Feitsma's list; it is
+// the verification that makes BPSW a deterministic test in that range).  About
+// 3.5 Miller-Rabin rounds of work per prime instead of the seven bases of
+// is_prime_mr, which remains the answer when no Lucas parameter is found.
 __device__ bool is_prime_bpsw(u64 n)
 {
     if (n < MR_BOUND) return true;        // sieve survivor below 65537^2

@@ -10,6 +10,8 @@ brute-force term oracle (oracle/_build/liboracle.so), on seeded inputs:
 
   setup_ref.npz    per-prime setup rows, kdata and sort outputs of the
                    reference kernels for six small jobs (b = 2,3,5,6,7,10)
+                   at p < 4000, and for five jobs at p from 2^50 and just
+                   below 2^64 (among them the config-2 and config-4 n-ranges)
   verify_ref.json  verify_factor results (factors, non-factors, composite p)
   sprp2_ref.json   base-2 strong-PRP verdicts, and the composite numbers the
                    reference's 2-PRP generator admits in [3, 2e5)
@@ -32,6 +34,16 @@ from oracle import pyoracle as O  # noqa: E402
 from rssieve_b200 import workloads as W  # noqa: E402
 
 SETUP_JOBS = [(101, 2, 8), (102, 3, 8), (103, 5, 10), (104, 6, 8), (105, 7, 6), (106, 10, 12)]
+# the same rows where the Montgomery carries matter: primes from 2^50 (the
+# config-2 p-range) and just below 2^64 (config 4), on small n-ranges and on
+# the configurations' own n-ranges.  tag: seed, base, kcount, nmin, nmax, plo, kmax, k parity
+SETUP_JOBS_HIGH = {
+    "p2e50_b2": (111, 2, 8, 1000, 5000, 1 << 50, 1 << 31, 1),
+    "cfg2_b2": (112, 2, 16, 4000000, 9999999, (1 << 50) + (1 << 37), 1 << 31, 1),
+    "p2e64_b5": (113, 5, 10, 1000, 5000, (1 << 64) - (1 << 20), 1 << 31, 0),
+    "cfg4_b5": (114, 5, 20, 1000000, 2999999, (1 << 64) - (1 << 36), 1 << 31, 0),
+    "p2e64_b3": (115, 3, 12, 20000, 80000, (1 << 64) - (1 << 24), 1 << 31, 0),
+}
 BRUTE_JOBS = [  # seed, base, kcount, nmin, nmax, keep, p0, p1
     (201, 2, 8, 1000, 6000, 0.4, 3, 200000),
     (202, 3, 6, 2000, 5000, 0.5, 3, 150000),
@@ -57,6 +69,32 @@ def make_setup():
         out[tag + "_k"] = np.array(j["k"], dtype=np.uint64)
         out[tag + "_c"] = np.array(j["c"], dtype=np.int32)
         out[tag + "_nminmax"] = np.array([j["nmin"], j["nmax"], Q], dtype=np.uint32)
+        out[tag + "_primes"] = pl
+        out[tag + "_rows"] = r["rows"]
+        out[tag + "_kd_hadj"] = r["kd"]["hadj"]
+        out[tag + "_kd_parity"] = r["kd"]["parity"]
+        out[tag + "_kd_kidx"] = r["kd"]["kidx"]
+        out[tag + "_counts"] = r["counts"]
+        out[tag + "_rows_cls"] = r["rows_cls"]
+        out[tag + "_kcounts"] = r["kcounts"]
+    for tag, (seed, base, kc, nmin, nmax, plo, kmax, kpar) in SETUP_JOBS_HIGH.items():
+        g = W.SplitMix64(seed)
+        ks = []
+        while len(ks) < kc:
+            k = g.uniform(2, kmax)
+            k = (k | 1) if kpar else ((k & ~1) or 2)
+            if k not in ks:
+                ks.append(k)
+        cs = [1 if g.next() & 1 else -1 for _ in range(kc)]
+        words = (nmax - nmin + 1 + 31) // 32
+        oj = O.Job(base, ks, cs, nmin, nmax, np.zeros((kc, words), np.uint32))
+        pl = O.prp2(plo, min(plo + 200000, (1 << 64) - 1))[:300]
+        Q = O.ref_params(nmin, nmax)["Q"]
+        r = O.ref_setup_sort(oj, Q, 1024, pl)
+        out[tag + "_base"] = np.array([base], dtype=np.uint32)
+        out[tag + "_k"] = np.array(ks, dtype=np.uint64)
+        out[tag + "_c"] = np.array(cs, dtype=np.int32)
+        out[tag + "_nminmax"] = np.array([nmin, nmax, Q], dtype=np.uint32)
         out[tag + "_primes"] = pl
         out[tag + "_rows"] = r["rows"]
         out[tag + "_kd_hadj"] = r["kd"]["hadj"]
@@ -144,7 +182,7 @@ def make_abcd():
 
 
 if __name__ == "__main__":
-    O.build()
+    O.build(os.environ.get("RSSIEVE_REFERENCE_DIR"))
     assert O.ref_available(), "oracle/_ref/librsref.so is needed (build it where the reference tree exists)"
     make_setup()
     make_verify()

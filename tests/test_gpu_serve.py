@@ -1,7 +1,8 @@
 """Serving loop: units arrive over time and share the device (continuous batching).
 
-Each unit's eliminated terms and final bitmap must be the same in the mix as
-when the unit runs alone (the single-job path on the same file and p-range):
+Each unit's eliminated terms and final bitmap must equal the brute-force
+oracle's over the unit's file and p-range, and be the same in the mix as when
+the unit runs alone (the single-job path on the same file and p-range):
 units are device-side clones of their file's resident template, each with its
 own bitmap.  At most four units run at once, so later arrivals wait for slots
 and are admitted while earlier ones are still running.
@@ -11,6 +12,7 @@ import pytest
 
 from rssieve_b200 import serve
 from rssieve_b200 import workloads as W
+from tests.conftest import oracle_job
 
 pytestmark = pytest.mark.gpu
 
@@ -25,7 +27,7 @@ def _terms(f):
     return set(zip(f["seq"].tolist(), f["n"].tolist()))
 
 
-def test_units_same_alone_and_in_the_mix(rs, sieve):
+def test_units_same_alone_and_in_the_mix(rs, sieve, oracle):
     files = _files()
     seqs = [W.seqs_of(f) for f in files]
     g = np.random.default_rng(9)
@@ -41,6 +43,10 @@ def test_units_same_alone_and_in_the_mix(rs, sieve):
     assert all(u.finished is not None and u.admitted >= u.arrival for u in done)
     assert any(u.admitted > u.arrival for u in done)       # some waited for a slot
     for u in done:
+        # against the brute-force oracle: the unit's file over its own p-range
+        ofac, _, obm = oracle.brute(oracle_job(oracle, files[u.file]), oracle.primes(u.p0, u.p1), ref_skip=True)
+        assert _terms(u.factors) == _terms(ofac), u.uid
+        assert np.array_equal(u.bitmap, obm), u.uid
         sieve.load(seqs[u.file])
         cnt = sieve.run(u.p0, u.p1)
         f = sieve.factors()

@@ -160,7 +160,7 @@ def test_checkpoint_is_byte_compatible_with_reference_layout(rs, tmp_path):
     st.write(str(path), s)
     want = _ref_state_bytes(3, 10 ** 9, 123456789, 77, 5000, 4, 1700000000, 9, 1000, 2000, 2, [91549, -131179])
     assert path.read_bytes() == want
-    back = rs.State.read(str(path), s)
+    back = rs.State.read(str(path), s, 3, 10 ** 9)
     assert (back.p, back.checksum, back.primecount, back.factorcount, back.dupcount) == (123456789, 77, 5000, 4, 9)
 
 
@@ -173,16 +173,19 @@ def test_checkpoint_rejects_corrupt_truncated_and_foreign(rs, tmp_path):
     raw[20] ^= 1                                            # flip a bit in p
     path.write_bytes(bytes(raw))
     with pytest.raises(rs.RSError) as e:
-        rs.State.read(str(path), s)
+        rs.State.read(str(path), s, 3, 10 ** 9)
     assert e.value.code == rs.RS_ESTATE and "Checksum" in str(e.value)
     st.write(str(path), s)
     path.write_bytes(path.read_bytes()[:100])               # truncated
     with pytest.raises(rs.RSError):
-        rs.State.read(str(path), s)
+        rs.State.read(str(path), s, 3, 10 ** 9)
     st.write(str(path), s)
     other = rs.Seqs.create(2, [91549, 131179], [1, -1], 1000, 2002)
     with pytest.raises(rs.RSError):                         # another job's checkpoint
-        rs.State.read(str(path), other)
+        rs.State.read(str(path), other, 3, 10 ** 9)
+    with pytest.raises(rs.RSError) as e:                    # another p-range's checkpoint
+        rs.State.read(str(path), s, 3, 10 ** 9 + 2)
+    assert e.value.code == rs.RS_ESTATE and "Invalid checkpoint" in str(e.value)
 
 
 def test_checkpoint_v2_for_64bit_k(rs, tmp_path):
@@ -191,31 +194,63 @@ def test_checkpoint_v2_for_64bit_k(rs, tmp_path):
     path = tmp_path / "s.ckp"
     st.write(str(path), s)
     assert path.read_bytes()[:6] == b"RSB200"
-    back = rs.State.read(str(path), s)
+    back = rs.State.read(str(path), s, 2 ** 63, 2 ** 64 - 1)
     assert back.p == 2 ** 63 + 5 and back.dupcount == 3
 
 
 def test_resume_newest_wins_and_tie_goes_to_b(rs, tmp_path):
     s = rs.Seqs.create(2, [3], [1], 10, 20)
     a, b = str(tmp_path / "stateA.ckp"), str(tmp_path / "stateB.ckp")
-    assert rs.State.resume(a, b, s) == (None, -1)
+    assert rs.State.resume(a, b, s, 3, 1000) == (None, -1)
     rs.State(pmin=3, pmax=1000, p=500).write(a, s)
-    st, which = rs.State.resume(a, b, s)
+    st, which = rs.State.resume(a, b, s, 3, 1000)
     assert which == 0 and st.p == 500
     rs.State(pmin=3, pmax=1000, p=700).write(b, s)
-    st, which = rs.State.resume(a, b, s)
+    st, which = rs.State.resume(a, b, s, 3, 1000)
     assert which == 1 and st.p == 700
     rs.State(pmin=3, pmax=1000, p=900).write(a, s)
-    st, which = rs.State.resume(a, b, s)
+    st, which = rs.State.resume(a, b, s, 3, 1000)
     assert which == 0 and st.p == 900
     rs.State(pmin=3, pmax=1000, p=900).write(b, s)
-    st, which = rs.State.resume(a, b, s)
+    st, which = rs.State.resume(a, b, s, 3, 1000)
     assert which == 1
     with open(b, "r+b") as fh:                               # corrupt B: A is used
         fh.seek(40)
         fh.write(b"\xff")
-    st, which = rs.State.resume(a, b, s)
+    st, which = rs.State.resume(a, b, s, 3, 1000)
     assert which == 0 and st.p == 900
+
+
+def test_resume_ignores_a_newer_file_of_another_p_range(rs, tmp_path):
+    """A good A for this run and a stale B of another p-range with a larger p:
+    B is invalid before the two are compared, so A is resumed (read_state,
+    cl_sieve.cpp:236-242,288-318), not a fresh start that truncates the factors."""
+    s = rs.Seqs.create(2, [3], [1], 10, 20)
+    a, b = str(tmp_path / "stateA.ckp"), str(tmp_path / "stateB.ckp")
+    rs.State(pmin=3, pmax=1000, p=500).write(a, s)
+    rs.State(pmin=3, pmax=5000, p=4000).write(b, s)
+    st, which = rs.State.resume(a, b, s, 3, 1000)
+    assert which == 0 and st.p == 500 and st.pmax == 1000
+    assert rs.State.resume(a, b, s, 3, 5000)[1] == 1         # B is the valid one for its own range
+    assert rs.State.resume(a, b, s, 7, 1000) == (None, -1)
+
+
+def test_cli_resumes_from_the_file_of_its_own_range(rs, tmp_path):
+    """The command line with a valid A and a stale B of a wider range: it must
+    resume from A and keep the factor file (checked before any device work: the
+    checkpoint says the range is complete)."""
+    import subprocess
+    abcd = tmp_path / "in.txt"
+    abcd.write_text("ABCD 3*2^$a+1 [11]\n4\n")
+    s = rs.Seqs.create(2, [3], [1], 10, 15)
+    rs.State(pmin=100, pmax=1000, p=1000).write(str(tmp_path / "stateA.ckp"), s)
+    rs.State(pmin=100, pmax=9000, p=5000).write(str(tmp_path / "stateB.ckp"), s)
+    (tmp_path / "psp_sr2sieve.out").write_text("kept\n")
+    r = subprocess.run([rs.CLI_PATH, "-i", str(abcd), "-p", "100", "-P", "1000"], capture_output=True, text=True,
+                       cwd=tmp_path)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Resuming from checkpoint in stateA.ckp" in r.stdout and "Workunit complete" in r.stdout
+    assert (tmp_path / "psp_sr2sieve.out").read_text() == "kept\n"
 
 
 def test_cli_argument_errors(rs, tmp_path):

@@ -52,6 +52,55 @@ def test_setup_fixture_against_live_reference(oracle, base):
     assert np.array_equal(r["kcounts"], g[tag + "_kcounts"])
 
 
+HIGH_TAGS = ["p2e50_b2", "cfg2_b2", "p2e64_b5", "cfg4_b5", "p2e64_b3"]
+
+
+@pytest.mark.parametrize("tag", HIGH_TAGS)
+def test_setup_restatement_at_high_p(oracle, tag):
+    """The same value-for-value check where the Montgomery carries matter:
+    primes from 2^50 and just below 2^64, including the config-2 and config-4
+    n-ranges (the reference's own setup.cl rows and kdata as fixtures)."""
+    g = np.load(os.path.join(GOLD, "setup_ref.npz"))
+    base = int(g[tag + "_base"][0])
+    job = _job(oracle, g, tag, base)
+    Q = int(g[tag + "_nminmax"][2])
+    pl = g[tag + "_primes"]
+    assert int(pl[0]) >= 1 << 50
+    rows, kd = oracle.setup(job, Q, pl)
+    assert np.array_equal(rows, g[tag + "_rows"])
+    assert np.array_equal(kd["hadj"], g[tag + "_kd_hadj"])
+    assert np.array_equal(kd["parity"], g[tag + "_kd_parity"])
+    assert np.array_equal(kd["kidx"], g[tag + "_kd_kidx"])
+    assert int((g[tag + "_rows"][:, 0] != 0).sum()) > 200          # most primes searched, not skipped
+
+
+@pytest.mark.parametrize("tag", HIGH_TAGS)
+def test_high_p_setup_fixture_against_live_reference(oracle, tag):
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built here")
+    g = np.load(os.path.join(GOLD, "setup_ref.npz"))
+    job = _job(oracle, g, tag, int(g[tag + "_base"][0]))
+    r = oracle.ref_setup_sort(job, int(g[tag + "_nminmax"][2]), 1024, g[tag + "_primes"])
+    assert np.array_equal(r["rows"], g[tag + "_rows"])
+    assert np.array_equal(r["kd"]["hadj"], g[tag + "_kd_hadj"])
+    assert np.array_equal(r["counts"], g[tag + "_counts"])
+    assert np.array_equal(r["rows_cls"], g[tag + "_rows_cls"])
+    assert np.array_equal(r["kcounts"], g[tag + "_kcounts"])
+
+
+def test_plant_helper_places_real_factors(oracle):
+    """The planted-factor helper used by the GPU tests: every (k, n) it returns
+    is a term that p divides, within the asked range and k bound."""
+    for p in oracle.primes(1 << 50, (1 << 50) + 3000)[:10].tolist():
+        for c in (1, -1):
+            r = oracle.plant(p, 2, c, 4000000, 10000000, 1 << 32, 1)
+            assert r is not None
+            k, n = r
+            assert k < 1 << 32 and k & 1 and 4000000 <= n < 10000000
+            assert (k * pow(2, n, p) + c) % p == 0
+            assert oracle.verify_factor(p, k, n, c, 2) == 1
+
+
 def test_verify_matches_reference_verify_factor(oracle, rs):
     v = json.load(open(os.path.join(GOLD, "verify_ref.json")))
     for case, want in zip(v["cases"], v["ref_result"]):
