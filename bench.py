@@ -267,6 +267,59 @@ def measure_one_job_batched(torch, rs, W, peak_g, job, p0, width_log2, nsplit, l
             "identical_eliminated_terms": bool(same), "baby_steps_used": q}
 
 
+def measure_config1(torch, rs, W, peak_g):
+    """Config 1 end to end (8 sequences k*2^n-1, k < 2^20, n in [1e5, 3e5), the
+    whole p-range [1e12, 1e12+1e8)): the GPU through the C ABI (upload, every
+    prime, factors back) beside the CPU port of the reference algorithm on every
+    host thread over the same range; term sets compared between the two, and
+    with the brute-force oracle on the first 2e6 of the range."""
+    import numpy as np
+    from oracle import pyoracle as O
+    job = W.config1(1)
+    seqs = W.seqs_of(job)
+    p0, p1 = job["prange"]
+    st = torch.cuda.Stream()
+    sv = rs.Sieve(torch.cuda.current_device())
+    sv.set_stream(st.cuda_stream)
+    sv.load(seqs)
+    sv.run(p0, p1)                             # the tuner settles this job shape's Q
+    sv.factors()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record(st)
+    sv.load(seqs)
+    c = sv.run(p0, p1)
+    f = sv.factors()
+    ev[1].record(st)
+    torch.cuda.synchronize()
+    gms = ev[0].elapsed_time(ev[1])
+    q, _ = sv.baby_steps()
+    gpu_terms = O.term_set(f)
+    sub = sv
+    sub.load(seqs)
+    sub.run(p0, p0 + 2_000_000)
+    fsub = sub.factors()
+    sv.close()
+    oj = O.Job(job["base"], job["k"], job["c"], job["nmin"], job["nmax"], job["bitmap"])
+    threads = os.cpu_count() or 1
+    pl = O.prp2(p0, p1)
+    t = time.perf_counter()
+    pf, pst, _ = O.bsgs(oj, pl, nthreads=threads)
+    cdt = time.perf_counter() - t
+    bf, _, _ = O.brute(oj, O.primes(p0, p0 + 2_000_000))
+    return {"workload": "config1: 8 seqs k*2^n-1, k odd < 2^20, n in [1e5,3e5) kept w.p. 0.06, "
+                        "p in [1e12, 1e12+1e8), whole range",
+            "primes": int(c["primes"]), "baby_steps_used": q,
+            "gpu_e2e_primes_per_s": c["primes"] / (gms / 1e3), "gpu_e2e_s": gms / 1e3,
+            "cpu_port_primes_per_s": len(pl) / cdt, "cpu_port_s": cdt, "cpu_port_cores": threads,
+            "cpu_port_prime_set": "base-2 strong probable primes (the reference's)",
+            "gpu_over_cpu_port": (c["primes"] / (gms / 1e3)) / (len(pl) / cdt),
+            "factors": len(gpu_terms),
+            "identical_eliminated_terms_gpu_vs_port": gpu_terms == O.term_set(pf),
+            "identical_eliminated_terms_gpu_vs_brute_first_2e6": O.term_set(fsub) == O.term_set(bf),
+            "mulmods": {"gpu": mulmod_rates(c, gms / 1e3, peak_g)}}
+
+
 def measure_served(rs, W, serve, peak_g, seed=5, nunits=60, rate=8.0, width_log2=(22, 26)):
     """Config-5 shape, scaled down: 16 config-2-style files, Poisson arrivals at `rate`
     units/s, unit widths 2^22..2^26 (the full workload's are 2^30..2^36); latency
@@ -362,6 +415,8 @@ def main():
     sv = rs.Sieve(local)
     sv.set_stream(stream.cuda_stream)
     peak = sv.mulmod_peak()
+    wide = sv.widemul_peak()
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
     sv.set_baby_steps(args.baby_steps)
     sv.load(seqs)
     width = 1 << args.width
@@ -405,8 +460,11 @@ def main():
     value = primes_all / (dev_ms_max / 1e3)
     giant_all = sum_over_ranks(tot["giant"])
     bsgs_ms_avg = bsgs_ms / max(bsgs_launches, 1)
-    # roofline of the BSGS kernel: giant-step Montgomery products per launch / average launch time
-    achieved = (tot["giant"] / max(bsgs_launches, 1)) / (bsgs_ms_avg / 1e3) / 1e9
+    # roofline of the BSGS kernel: its executed steps per launch (baby steps and
+    # giant steps, one modular product -- or doublings for b^e <= 4 -- and one
+    # table insert or probe each) / average launch time
+    achieved = ((tot["giant"] + tot["baby"]) / max(bsgs_launches, 1)) / (bsgs_ms_avg / 1e3) / 1e9
+    peak_mult = wide / 11.0                       # products the 32x32->64 multiplier allows
     fac = sv.factors()
 
     e2e = None
@@ -447,7 +505,8 @@ def main():
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         from rssieve_b200 import serve
-        forms = {"batched": measure_batched(torch, rs, W, peak),
+        forms = {"config1": measure_config1(torch, rs, W, peak),
+                 "batched": measure_batched(torch, rs, W, peak),
                  "batched_config2": measure_one_job_batched(torch, rs, W, peak, job, P_START + (1 << 37), 29, 32,
                                                             "config2 job"),
                  "batched_config4": measure_one_job_batched(torch, rs, W, peak, W.config4(), (1 << 64) - (1 << 36),
@@ -482,7 +541,15 @@ def main():
                          "unit": "Gmulmod/s", "frac": achieved / peak,
                          "traffic": BSGS_DRAM_BYTES_PER_PRIME * tot["primes"] / max(bsgs_launches, 1),
                          "traffic_unit": "bytes per BSGS launch (ncu per-prime DRAM bytes x primes per launch)",
-                         "peak_source": "measured live: rs_mulmod_peak, independent Montgomery-product chains"},
+                         "work_unit": "baby + giant steps of the BSGS kernel (each one modular product or "
+                                      "doublings, plus one table insert or probe)",
+                         "peak_source": "measured live: rs_mulmod_peak, independent Montgomery-product chains",
+                         "peak_multiplier": peak_mult,
+                         "frac_of_multiplier_peak": achieved / peak_mult,
+                         "peak_multiplier_source": "measured live: rs_widemul_peak (independent mad.wide.u32 "
+                                                   "chains) / 11 wide products per Montgomery product",
+                         "r_wide_per_sm_clock": (wide * 1e9 / (sms * clocks["sm_mhz"] * 1e6)) if clocks else None,
+                         "giant_only_frac": (tot["giant"] / max(bsgs_launches, 1)) / (bsgs_ms_avg / 1e3) / 1e9 / peak},
             "cpu_baseline": cpu,
             "forms": forms,
             "clocks": clocks,

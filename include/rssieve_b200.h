@@ -67,7 +67,9 @@ typedef struct rs_counters {
     uint64_t primes;
     uint64_t skipped;           /* p | b, p | some k, or no solvable k */
     uint64_t full;              /* primes searched over every n */
-    uint64_t parity;            /* primes searched over one parity of n */
+    uint64_t parity;            /* primes searched over one class of n mod e per sequence, e >= 2
+                                   (e = 2 is the reference's parity split; larger e come from
+                                   power-residue characters of higher order) */
     uint64_t targets;           /* sum of surviving k over searched primes */
     uint64_t baby;              /* baby steps */
     uint64_t giant;             /* giant steps = Montgomery products + probes */
@@ -264,6 +266,12 @@ int rs_batch_counters(rs_batch *b, rs_counters *out);
  * on this device, in 10^9 products/s: the roofline denominator of the
  * integer-multiply-bound BSGS kernel. */
 int rs_mulmod_peak(rs_ctx *ctx, double *gmulmods_per_s, double *ms);
+/* Measured 32x32->64 multiply throughput of the device (10^9 wide products/s,
+ * sixteen independent mad.wide.u32 chains per thread).  A 64-bit Montgomery
+ * product takes 11 of them, so *gwide_per_s / 11 is the product rate the
+ * multiplier itself allows.  A measurement aid with no reference counterpart
+ * (the reference reports no roofline). */
+int rs_widemul_peak(rs_ctx *ctx, double *gwide_per_s, double *ms);
 
 /* Largest range width (p1 - p0) that rs_primes_generate_noalloc accepts. */
 #define RS_NOALLOC_MAX_WIDTH (1ull << 22)

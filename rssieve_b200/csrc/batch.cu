@@ -116,7 +116,7 @@ struct rs_batch {
     PrimeHdr *d_hdr = nullptr;
     void *d_aux = nullptr;
     u64 *d_tabs = nullptr, *d_tgt = nullptr;
-    unsigned char *d_meta = nullptr;
+    unsigned short *d_meta = nullptr;
     u32 *d_err = nullptr;
     u64 *d_stats = nullptr;
     u32 *d_unfinished = nullptr;
@@ -212,11 +212,11 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         !alloc(&b->d_aux, (size_t)R * RCAP * setup_aux_bytes()) ||
         !alloc((void **)&b->d_tabs, (size_t)R * RCAP * TABS * 8) ||
         !alloc((void **)&b->d_tgt, (size_t)R * RCAP * KSTRIDE * 8) ||
-        !alloc((void **)&b->d_meta, (size_t)R * RCAP * KSTRIDE) || !alloc((void **)&b->d_win, R * 4) ||
+        !alloc((void **)&b->d_meta, (size_t)R * RCAP * KSTRIDE * 2) || !alloc((void **)&b->d_win, R * 4) ||
         !alloc((void **)&b->d_prefix_c, (R + 1) * 4) || !alloc((void **)&b->d_prefix_p, (R + 1) * 4) ||
         cudaMallocHost(&b->h_pin, 16) != cudaSuccess || cudaMallocHost(&b->h_win_pin, R * 4) != cudaSuccess) {
         rs_set_error("cannot allocate a batch of %u range slots (about %zu MB)", R,
-                     (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 9 + 24 + 8 + 16) >> 20);
+                     (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 10 + 24 + 8 + 16) >> 20);
         return fail(RS_ENOMEM);
     }
     if (cudaMemcpy(b->d_sp, sp.data(), sp.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -357,15 +357,10 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
     }
     J.jd.bitmap = J.d_bitmap;
     J.used = true;
-    const BsgsGeom &g = BSGS_GEOMS[J.geom];
-    JobGeom G;
-    G.q = g.q; G.c = g.c; G.tpb = g.tpb; G.pad_ = 0;
-    G.m1 = (u32)(((u64)J.jd.L + g.q - 1) / g.q);
-    G.m2 = (u32)(((u64)J.jd.L + 2ull * g.q - 1) / (2ull * g.q));
+    const JobGeom G = job_geom(J.geom);
     BsgsArgs A;
     memset(&A, 0, sizeof A);
     A.base = J.jd.base; A.nmin = J.jd.nmin; A.nmax = J.jd.nmax; A.words = J.jd.words;
-    A.M1 = G.m1; A.M2 = G.m2;
     A.bitmap = J.d_bitmap;
     A.factors = J.d_factors;
     A.factor_ctr = b->d_fctrs + jid;
@@ -486,7 +481,7 @@ static int batch_round(rs_batch *b)
     BCU(launch_mr_batch(b->d_cands, CCAP, b->d_primes, RCAP, b->d_ctrs, R, b->d_prefix_c, b->d_err, b->sms, st));
     BCU(launch_batch_prefix_all(b->d_ranges, R, 1, RCAP, b->d_ctrs, b->d_prefix_p, st));
     BCU(launch_setup_batch(b->d_jobs, b->d_geoms, b->d_ranges, b->d_primes, RCAP, b->d_prefix_p, R, b->d_hdr,
-                           b->d_aux, b->d_tabs, b->d_tgt, b->d_meta, b->d_stats, b->sms, st));
+                           b->d_aux, b->d_tabs, b->d_tgt, b->d_meta, b->d_stats, b->d_err, b->sms, st));
     BsgsArgs a;
     memset(&a, 0, sizeof a);
     a.stats = b->d_stats;

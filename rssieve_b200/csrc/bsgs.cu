@@ -7,11 +7,13 @@
 //                steps (additions when b^e <= 16), checks y_j == 1 to detect
 //                ord(s) < Q (giant.cl:123-134), then inserts j < ord into a
 //                shared-memory hash table.
-//   giant phase  gamma = T_i * S^q for q in [0,M): thread (i,g) walks q in
+//   giant phase  gamma = T_i * S^q for q in [0,Mg): thread (i,g) walks q in
 //                [g*Lc, (g+1)*Lc) from T_i * S^(g*Lc) as two interleaved
 //                chains, one modular product (Shoup's for p < 2^63, else
 //                Montgomery) and one table probe per step (giant.cl:170-192).  A match
-//                s^j == gamma gives n = nmin + off_i + e*((q+1)*Q - 1 - j).
+//                s^j == gamma gives n = nmin + off_i + e*((q+1)*Q - 1 - j),
+//                where s = b^e and off_i is target i's class of n mod e
+//                (setup.cu; e = 2 is the reference's parity split).
 //   small order  ord(s) < Q: each target is looked up once and every n in
 //                range with the same residue mod e*ord is claimed (giant.cl:146-168).
 //   claims       atomicAnd on the term's bitmap bit; the first claimer appends
@@ -164,7 +166,7 @@ struct RecBuf {
     PrimeHdr hdr;
     u64 tabs[TABS];                 // A[32] B[32] Z1[32] Z2[32]
     u64 tgt[KSTRIDE];
-    unsigned char meta[KSTRIDE];
+    unsigned short meta[KSTRIDE];   // sequence | offset << 7
 };
 static_assert(sizeof(RecBuf) % 16 == 0, "bulk copies move 16-byte units");
 
@@ -389,7 +391,7 @@ __device__ __forceinline__ u32 batch_slot(u32 i, u32 nr, const u32 *prefix, u32 
 template <int TPB, int C, int NB, int MODE, bool BATCH>
 __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const PrimeHdr *__restrict__ hdr,
                                                  const u64 *__restrict__ tabs, const u64 *__restrict__ tgt,
-                                                 const unsigned char *__restrict__ meta, u32 count, u32 *work_ctr,
+                                                 const unsigned short *__restrict__ meta, u32 count, u32 *work_ctr,
                                                  const BsgsArgs *__restrict__ job_args, u32 nr,
                                                  const u32 *__restrict__ prefix, u32 rcap)
 {
@@ -418,7 +420,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         bulk_load(&r->hdr, hdr + idx, (u32)sizeof(PrimeHdr), &s_bar[buf]);
         bulk_load(r->tabs, tabs + (size_t)idx * TABS, TABS * 8, &s_bar[buf]);
         bulk_load(r->tgt, tgt + (size_t)idx * KSTRIDE, KSTRIDE * 8, &s_bar[buf]);
-        bulk_load(r->meta, meta + (size_t)idx * KSTRIDE, KSTRIDE, &s_bar[buf]);
+        bulk_load(r->meta, meta + (size_t)idx * KSTRIDE, KSTRIDE * 2, &s_bar[buf]);
     };
     u64 st_baby = 0, st_giant = 0, st_small = 0;                  // thread 0's tallies
     if (tid == 0) {
@@ -492,9 +494,13 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             // The step kind is uniform per prime (b^e = 2, 4 or other) and is
             // chosen once, so the loop body carries no dispatch; the first j > 0
             // with y_j = 1 is kept per thread and merged with one atomicMin.
+            // Other multipliers take Shoup's product by the plain s below 2^63
+            // (the same residues as the Montgomery product verify() uses).
             u32 minj = 0xFFFFFFFFu;
+            const u64 ssw = R.hdr.ssw;
+            const u64 sp = (MODE == 1 && smul != 2 && smul != 4) ? from_mont(s, Mont{p, q, 0, 0}) : 0;
             auto babies = [&](auto kind) {
-                constexpr int K = decltype(kind)::value;          // b^e = 2 or 4 (doublings), else 0
+                constexpr int K = decltype(kind)::value;          // 2, 4: doublings; 1: Shoup; 0: baby_step
 #pragma unroll
                 for (int h0 = 0; h0 < C; h0 += IB) {
                     u32 bk[IB], fp[IB], old[IB];
@@ -504,6 +510,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                         if (j != 0 && x == one && minj == 0xFFFFFFFFu) minj = j;
                         tab_hash<NB>(x, bk[i], fp[i]);
                         if (K == 0) x = baby_step(x, smul, s, p, q);
+                        else if (K == 1) x = shoup_mul(x, sp, ssw, p);
                         else if (MODE == 1) { x = dbl63(x, p); if (K == 4) x = dbl63(x, p); }
                         else { x = madd(x, x, p); if (K == 4) x = madd(x, x, p); }
                     }
@@ -518,13 +525,14 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             };
             if (smul == 2) babies(std::integral_constant<int, 2>{});
             else if (smul == 4) babies(std::integral_constant<int, 4>{});
+            else if (MODE == 1) babies(std::integral_constant<int, 1>{});
             else babies(std::integral_constant<int, 0>{});
             if (minj != 0xFFFFFFFFu) atomicMin(&s_order, minj);
             if (spill) s_spill = 1;
         }
         __syncthreads();
         const u32 order = s_order;
-        const u32 Mg = (e == 2) ? s_args.M2 : s_args.M1;
+        const u32 Mg = R.hdr.Mg;
         if (live) {
             if (order < Q) rebuild_table<TPB, C, NB>(order);
             else if (tid == 0 && s_spill) atomicOr(a.err, ERR_HASH_OVERFLOW);
@@ -600,7 +608,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
 
 template <int G, int MODE, bool BATCH = false>
 static cudaError_t launch_geom(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
-                              const unsigned char *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st,
+                              const unsigned short *meta, u32 count, u32 *work_ctr, int sms, cudaStream_t st,
                               const BsgsArgs *job_args = nullptr, u32 nr = 0, const u32 *prefix = nullptr,
                               u32 rcap = 0)
 {
@@ -660,7 +668,7 @@ cudaError_t bsgs_prepare()
 }
 
 cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
-                        const unsigned char *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int geom, int sms,
+                        const unsigned short *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int geom, int sms,
                         cudaStream_t st)
 {
     if (count == 0) return cudaSuccess;
@@ -731,7 +739,7 @@ cudaError_t launch_batch_prefix_all(const BatchRange *ranges, u32 nr, int which,
 }
 
 cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
-                              const u64 *tgt, const unsigned char *meta, u32 nr, const u32 *prefix, u32 rcap,
+                              const u64 *tgt, const unsigned short *meta, u32 nr, const u32 *prefix, u32 rcap,
                               u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st)
 {
 #define RS_BSGS_BCASE(G)                                                                                         \

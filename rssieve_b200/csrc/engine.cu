@@ -43,7 +43,7 @@ struct rs_ctx {
     void *d_aux = nullptr;
     u64 *d_tabs = nullptr;
     u64 *d_tgt = nullptr;
-    unsigned char *d_meta = nullptr;
+    unsigned short *d_meta = nullptr;
     // job
     bool job_loaded = false;
     JobDev h_job;
@@ -169,7 +169,7 @@ extern "C" int rs_ctx_create(int device, rs_ctx **out)
         cudaMalloc(&c->d_aux, (size_t)c->chunk_cap * setup_aux_bytes()) != cudaSuccess ||
         cudaMalloc(&c->d_tabs, (size_t)c->chunk_cap * TABS * 8) != cudaSuccess ||
         cudaMalloc(&c->d_tgt, (size_t)c->chunk_cap * KSTRIDE * 8) != cudaSuccess ||
-        cudaMalloc(&c->d_meta, (size_t)c->chunk_cap * KSTRIDE) != cudaSuccess ||
+        cudaMalloc(&c->d_meta, (size_t)c->chunk_cap * KSTRIDE * 2) != cudaSuccess ||
         cudaMalloc(&c->d_job, sizeof(JobDev)) != cudaSuccess ||
         cudaMallocHost(&c->h_pin, 64) != cudaSuccess) {
         rs_set_error("device allocation failed");
@@ -192,13 +192,6 @@ extern "C" int rs_ctx_set_stream(rs_ctx *c, void *stream)
     if (!c) return RS_EARG;
     c->stream = stream ? (cudaStream_t)stream : c->own;
     return RS_OK;
-}
-
-static void odd_split(u64 x, u64 &odd, u32 &v2)
-{
-    v2 = 0;
-    while (!(x & 1)) { x >>= 1; ++v2; }
-    odd = x;
 }
 
 // Jobs of one shape share a tuned geometry (a reloaded or resumed job skips
@@ -300,8 +293,7 @@ extern "C" int rs_get_baby_steps(rs_ctx *c, uint32_t *q, int *tuning)
     return RS_OK;
 }
 
-// Device record of a job: sequences, n-range, odd parts and Barrett
-// reciprocals of every k and of the base (bitmap pointer left null).
+// Device record of a job: sequences and n-range (bitmap pointer left null).
 void jobdev_from_seqs(const rs_seqs *s, JobDev *out)
 {
     memset(out, 0, sizeof *out);
@@ -314,11 +306,7 @@ void jobdev_from_seqs(const rs_seqs *s, JobDev *out)
     for (u32 i = 0; i < s->kcount; ++i) {
         out->k[i] = s->k[i];
         out->c[i] = s->c[i];
-        odd_split(s->k[i], out->kodd[i], out->kv2[i]);
-        out->krd[i] = ~0ull / out->kodd[i];
     }
-    odd_split(s->base, out->bodd, out->bv2);
-    out->brd = ~0ull / out->bodd;
 }
 
 extern "C" int rs_job_load(rs_ctx *c, const rs_seqs *s)
@@ -520,11 +508,8 @@ extern "C" int rs_run_range(rs_ctx *c, uint64_t p0, uint64_t p1, rs_counters *de
             // while tuning, full chunks cycle through the candidate geometries
             const int g = (c->tuning && cnt >= 32768) ? c->tune_cand[c->tune_next++ % c->tune_ncand] : c->geom;
             c->chunk_geom[ci] = g;
-            const u32 Q = BSGS_GEOMS[g].q;
-            a.M1 = (u32)(((u64)c->h_job.L + Q - 1) / Q);
-            a.M2 = (u32)(((u64)c->h_job.L + 2ull * Q - 1) / (2ull * Q));
             CU(launch_setup(c->d_job, c->d_primes, first, cnt, c->d_hdr, c->d_aux, c->d_tabs, c->d_tgt, c->d_meta,
-                            c->d_stats, g, c->h_job.L, c->stream));
+                            c->d_stats, c->d_err, g, c->stream));
             CU(cudaMemsetAsync(c->d_ctrs + 2, 0, 4, c->stream));
             CU(cudaEventRecord(c->ev[2 + 2 * ci], c->stream));
             CU(launch_bsgs(a, c->d_hdr, c->d_tabs, c->d_tgt, c->d_meta, cnt, c->d_ctrs + 2, p, hi, g, c->sms,
@@ -610,6 +595,28 @@ extern "C" int rs_last_timing(rs_ctx *c, double *bsgs_ms, double *total_ms, uint
     if (total_ms) *total_ms = c->last_total_ms;
     if (bl) *bl = c->last_bsgs_launches;
     if (kl) *kl = c->last_kernel_launches;
+    return RS_OK;
+}
+
+extern "C" int rs_widemul_peak(rs_ctx *c, double *gwide_per_s, double *ms_out)
+{
+    if (!c || !gwide_per_s) return RS_EARG;
+    CU(cudaSetDevice(c->device));
+    const int blocks = c->sms * 8, iters = 8192;
+    u64 *out = nullptr;
+    CU(cudaMalloc(&out, (size_t)blocks * 256 * 8));
+    int rc = ensure_events(c, 2);
+    if (rc) { cudaFree(out); return rc; }
+    CU(launch_widemul_peak(out, blocks, 64, c->stream));          // warm-up
+    CU(cudaEventRecord(c->ev[0], c->stream));
+    CU(launch_widemul_peak(out, blocks, iters, c->stream));
+    CU(cudaEventRecord(c->ev[1], c->stream));
+    CU(cudaEventSynchronize(c->ev[1]));
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    cudaFree(out);
+    *gwide_per_s = (double)blocks * 256 * 16 * iters / (ms * 1e-3) / 1e9;
+    if (ms_out) *ms_out = ms;
     return RS_OK;
 }
 

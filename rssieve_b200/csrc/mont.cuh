@@ -145,23 +145,6 @@ RS_DEV u64 mul_base(u64 x, u32 b, u64 bm, const Mont &M)
 // Jacobi symbol (a/n) for odd n > 0 and 0 <= a < n: binary algorithm
 // (strip factors of two with the (2/n) rule, swap with quadratic
 // reciprocity, subtract).  Returns -1, 0 or 1.
-RS_DEV int jacobi64(u64 a, u64 n)
-{
-    int t = 1;
-    while (a) {
-        int z = __ffsll((long long)a) - 1;
-        a >>= z;
-        u32 r8 = (u32)n & 7;
-        if ((z & 1) && (r8 == 3 || r8 == 5)) t = -t;
-        if (a < n) {
-            u64 tmp = a; a = n; n = tmp;
-            if ((a & 3) == 3 && (n & 3) == 3) t = -t;
-        }
-        a -= n;
-    }
-    return (n == 1) ? t : 0;
-}
-
 RS_DEV int jacobi32(u32 a, u32 n)
 {
     int t = 1;
@@ -177,14 +160,4 @@ RS_DEV int jacobi32(u32 a, u32 n)
         a -= n;
     }
     return (n == 1) ? t : 0;
-}
-
-// x mod d with a precomputed rd = floor((2^64-1)/d), d >= 1 (Barrett; the
-// estimate is short by at most 2).
-RS_DEV u64 mod_barrett(u64 x, u64 d, u64 rd)
-{
-    u64 qe = __umul64hi(x, rd);
-    u64 r = x - qe * d;
-    while (r >= d) r -= d;
-    return r;
 }

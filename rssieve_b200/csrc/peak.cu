@@ -1,8 +1,10 @@
-// peak.cu -- the chip's Montgomery-product throughput, the roofline
-// denominator for the BSGS kernel.  Every thread runs eight independent
-// dependency chains of the same mmul() the kernels use (so the 32-bit IMAD
-// pipe, not latency, is the limit), on a 62-bit prime, for a fixed number of
-// steps; the rate is products / kernel time (CUDA events on the stream).
+// peak.cu -- the roofline denominators of the BSGS kernel, measured on the
+// device: the Montgomery-product throughput (every thread runs eight
+// independent dependency chains of the same mmul() the kernels use, so the
+// 32-bit IMAD pipe, not latency, is the limit, on a 62-bit prime) and the raw
+// 32x32->64 multiply throughput, from which the multiplier-bound product rate
+// is the wide-multiply rate / 11.  Rates are operations / kernel time (CUDA
+// events on the stream).
 #include "mont.cuh"
 #include "rs_internal.h"
 
@@ -22,6 +24,33 @@ __global__ void __launch_bounds__(256) k_mulmod_peak(u64 *out, u64 p, u64 q, u64
 #pragma unroll
     for (int j = 0; j < 8; ++j) x ^= a[j];
     out[t] = x;
+}
+
+// Wide-multiply throughput: sixteen independent chains per thread of one
+// 32x32->64 multiply-add each step, c = lo32(c) * m + c (mad.wide.u32, whose
+// low operand is the previous result, so nothing can be hoisted or folded).
+// A 64-bit Montgomery product needs 11 such products (a*b: 4, lo*q mod 2^64:
+// 3, hi(m*p): 4), so rate / 11 is the product rate the multiplier allows.
+__global__ void __launch_bounds__(256) k_widemul_peak(u64 *out, u32 m, int iters)
+{
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    u64 c[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) c[j] = t * 16ull + j + 1;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) c[j] = (u64)(u32)c[j] * m + c[j];
+    }
+    u64 x = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x ^= c[j];
+    out[t] = x;
+}
+
+cudaError_t launch_widemul_peak(u64 *out, int blocks, int iters, cudaStream_t st)
+{
+    k_widemul_peak<<<blocks, 256, 0, st>>>(out, 0x9E3779B1u, iters);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_mulmod_peak(u64 *out, int blocks, int iters, cudaStream_t st)

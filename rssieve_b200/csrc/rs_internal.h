@@ -19,7 +19,6 @@ typedef unsigned char u8;
 constexpr int KMAX = 100;            // sequences per job (inputfile.cpp:356-361)
 constexpr int KSTRIDE = 112;         // padded per-prime target stride (16-byte multiple for bulk copies)
 constexpr int TABS = 128;            // u64 power-table entries per prime
-constexpr int NDS = 12;              // power-residue degrees of setup.cl:22-48
 
 // BSGS kernel geometries: Q = tpb * c baby steps per prime, nb buckets of
 // seven slots (load about 0.4), 1024 / tpb CTAs per SM sharing its 228 KB of
@@ -42,14 +41,15 @@ constexpr int geom_index(u32 q)
 
 // Model cost of one prime for a geometry, in baby-step units: Q baby steps plus
 // the giant steps of the targets that survive the prefilter (about 0.6 of the
-// sequences; half the primes use the parity split, which halves their range),
-// a giant step costing about 1.2 baby steps, and the per-prime fixed work
-// (table clear, barriers) of about 0.15 Q.
+// sequences), each over one class of n modulo the prime's split modulus e
+// (ceil(L/(eQ)) steps, about 0.15 L/Q on average over primes, and at least
+// one), a giant step costing about 1.2 baby steps, and the per-prime fixed
+// work (table clear, barriers) of about 0.15 Q.
 inline double geom_model_cost(int g, u32 kcount, u32 L)
 {
     const double q = BSGS_GEOMS[g].q;
-    const double m = ((double)L + q - 1) / q;
-    return 1.15 * q + 1.2 * 0.6 * kcount * 0.75 * (double)(u64)m;
+    const double m = 0.15 * (double)L / q + 0.5;
+    return 1.15 * q + 1.2 * 0.6 * kcount * (m < 1.0 ? 1.0 : m);
 }
 inline int geom_model_best(u32 kcount, u32 L)
 {
@@ -81,13 +81,14 @@ constexpr u32 ERR_HASH_OVERFLOW = 4u;       // a bucket chain exceeded BSGS_MAXP
 constexpr u32 ERR_FACTOR_OVERFLOW = 8u;     // factor buffer full (cannot happen: sized to the bitmap)
 constexpr u32 ERR_TMA_TIMEOUT = 16u;        // a bulk copy did not complete within the wait bound
 constexpr u32 ERR_SIEVE_TABLE = 32u;        // the sieving-prime table is missing (does not start with 3)
+constexpr u32 ERR_SETUP_CLASS = 64u;        // a target passed the residue test but no class of n matched (cannot happen)
 
 // statistics counters (u64)
 enum Stat {
     ST_PRIMES = 0,        // primes generated (and tested)
     ST_SKIPPED,           // primes dividing b or some k, or with no solvable k (setup.cl:156-162,205-208)
-    ST_FULL,              // primes searched with a full-range table (b a quadratic residue)
-    ST_PARITY,            // primes searched with a parity table (b a non-residue)
+    ST_FULL,              // primes searched over every n (split modulus e = 1)
+    ST_PARITY,            // primes searched over one class of n mod e per sequence (e >= 2; e = 2: parity)
     ST_TARGETS,           // sum over primes of surviving k
     ST_BABY,              // baby steps executed
     ST_GIANT,             // giant steps executed (one Montgomery product and one lookup each)
@@ -106,30 +107,27 @@ struct JobDev {
     u32 words;           // bitmap words per sequence
     u64 k[KMAX];
     int c[KMAX];
-    u64 kodd[KMAX];      // odd part of k_i
-    u64 krd[KMAX];       // floor((2^64-1)/kodd)
-    u32 kv2[KMAX];       // 2-adic valuation of k_i
-    u64 bodd, brd;       // same for the base
-    u32 bv2;
-    u32 pad_;
     u32 *bitmap;         // kcount * words
 };
 
-struct PrimeHdr {        // 80 bytes (a 16-byte multiple: copied by TMA bulk copies)
+struct PrimeHdr {        // 96 bytes (a 16-byte multiple: copied by TMA bulk copies)
     u64 p;               // 0 = skipped
     u64 q;               // p^-1 mod 2^64
     u64 one;             // 2^64 mod p
-    u64 s;               // Montgomery b^e, e = 1 (full) or 2 (parity)
+    u64 s;               // Montgomery b^e, e = the split modulus (n runs over one class mod e per target)
     u64 S;               // Montgomery s^Q
     u32 numk;            // surviving targets
-    u32 e;               // 1 or 2
+    u32 e;               // split modulus, 1..64
     u32 G, Lc;           // giant phase: G chunks of Lc giant steps
     u32 smul;            // b^e as an integer when the baby step uses additions, else 0
     u32 job;             // job index within a batch (0 for a single job)
+    u32 Mg;              // giant steps per target: ceil(ceil(L/e)/Q)
+    u32 pad_;
     u64 Sh;              // Montgomery S^(Lc/2): start of a thread's second giant chain
     u64 Sw;              // floor(Sp*2^64/p), Sp = s^Q mod p (plain), for Shoup giant steps; 0 when p >= 2^63
+    u64 ssw;             // floor(sp*2^64/p), sp = s mod p (plain), for Shoup baby steps; 0 when p >= 2^63
 };
-static_assert(sizeof(PrimeHdr) == 80, "PrimeHdr is copied in 16-byte units");
+static_assert(sizeof(PrimeHdr) == 96, "PrimeHdr is copied in 16-byte units");
 
 struct FactorRec {       // one claimed term: p | k[seq]*b^n + c[seq]
     u64 p;
@@ -139,7 +137,6 @@ struct FactorRec {       // one claimed term: p | k[seq]*b^n + c[seq]
 
 struct BsgsArgs {
     u32 base, nmin, nmax, words;
-    u32 M1, M2;          // giant steps per target for this launch's Q: ceil(L/Q), ceil(L/(2Q))
     u32 *bitmap;
     FactorRec *factors;
     u32 *factor_ctr;
@@ -168,8 +165,17 @@ struct BatchRange {      // device state of one range slot
 constexpr int BR_CTRS = 4;
 // per-job BSGS geometry as the set-up kernels need it
 struct JobGeom {
-    u32 q, c, tpb, m1, m2, pad_;
+    u32 q, c, tpb, pad_;
 };
+inline JobGeom job_geom(int g)
+{
+    JobGeom G;
+    G.q = BSGS_GEOMS[g].q;
+    G.c = BSGS_GEOMS[g].c;
+    G.tpb = BSGS_GEOMS[g].tpb;
+    G.pad_ = 0;
+    return G;
+}
 
 // Index i of work spread over nr ranges with prefix sums prefix[0..nr]:
 // the range k with prefix[k] <= i < prefix[k+1] (i < prefix[nr]).
@@ -189,15 +195,16 @@ cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp,
 cudaError_t launch_mr(const u64 *cands, const u32 *ctrs, u32 cand_cap, u64 *primes, u32 prime_cap, u32 *prime_ctr,
                       u32 *err, int sms, cudaStream_t st);
 cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 count, PrimeHdr *hdr, void *aux, u64 *tabs,
-                         u64 *tgt, unsigned char *meta, u64 *stats, int geom, u32 L, cudaStream_t st);
+                         u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, int geom, cudaStream_t st);
 size_t setup_aux_bytes();
 // every prime of the launch lies in [pmin, pmax), entirely below or entirely at or above 2^63
 cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs, const u64 *tgt,
-                        const unsigned char *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int geom, int sms,
+                        const unsigned short *meta, u32 count, u32 *work_ctr, u64 pmin, u64 pmax, int geom, int sms,
                         cudaStream_t st);
 size_t bsgs_smem_bytes(int geom);
 cudaError_t bsgs_prepare();   // per device, before the first launch
 cudaError_t launch_mulmod_peak(u64 *out, int blocks, int iters, cudaStream_t st);
+cudaError_t launch_widemul_peak(u64 *out, int blocks, int iters, cudaStream_t st);
 
 // batch rounds (sieve.cu, setup.cu, bsgs.cu)
 // win[r]: primes range slot r should cover this round (0: none); capped at 0.6*rcap
@@ -212,7 +219,7 @@ cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u
 // set-up of the primes of all ranges (prefix_p: prefix sums of their counts)
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
                                u32 rcap, const u32 *prefix_p, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs,
-                               u64 *tgt, unsigned char *meta, u64 *stats, int sms, cudaStream_t st);
+                               u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, int sms, cudaStream_t st);
 // one BSGS launch per (geometry, mode) group over range slots [0, nr): prefix
 // (nr+1 entries) counts the primes of the active slots of that group only
 cudaError_t launch_batch_prefix(const BatchRange *ranges, u32 nr, int geom, bool shoup, const u32 *ctrs, u32 rcap,
@@ -221,7 +228,7 @@ cudaError_t launch_batch_prefix(const BatchRange *ranges, u32 nr, int geom, bool
 cudaError_t launch_batch_prefix_all(const BatchRange *ranges, u32 nr, int which, u32 cap, const u32 *ctrs,
                                     u32 *prefix, cudaStream_t st);
 cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
-                              const u64 *tgt, const unsigned char *meta, u32 nr, const u32 *prefix, u32 rcap,
+                              const u64 *tgt, const unsigned short *meta, u32 nr, const u32 *prefix, u32 rcap,
                               u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st);
 
 }  // namespace rs

@@ -1,24 +1,32 @@
 // setup.cu -- per-prime set-up for the BSGS search.
 //
 // Replaces the reference's setup and sort kernels (kernels/setup.cl:89-209,
-// kernels/sort.cl:11-104).  The arithmetic is re-derived rather than ported:
+// kernels/sort.cl:11-104).  The arithmetic is re-derived rather than ported.
 //
 // Term k*b^n + c (c = +-1) is divisible by p iff k*b^n == -c (mod p).  Write
-// n = nmin + off + e*u with e = 1 (b a quadratic residue mod p: one table for
-// every n) or e = 2 (b a non-residue: even n, off = 0, and odd n, off = 1,
-// share one table of powers of s = b^2), and u = (q+1)*Q - 1 - j with baby
-// index j in [0,Q) and giant index q.  Then
+// n = nmin + off + e*u with a split modulus e (one table of powers of s = b^e
+// serves every sequence) and u = (q+1)*Q - 1 - j with baby index j in [0,Q)
+// and giant index q.  Then
 //      s^j == T * S^q,   T = -c * k * b^(nmin + off + e*(Q-1)),   S = s^Q,
 // so the baby table holds s^j and no modular inverse is needed (the reference
 // batch-inverts every k and b^Q, setup.cl:133-166).
 //
-// The prefilter is the reference's (setup.cl:22-87), restated on k itself:
-// the target b^n == -c*k^-1 must be a d-th power whenever b is one (d | p-1,
-// d in {3,4,5,7,8,9,11,13,17,19,23,29}), i.e. k^((p-1)/d) == (-c)^((p-1)/d);
-// and its quadratic character (-c/p)(k/p), computed with Jacobi symbols instead
-// of an Euler power, decides impossible / full range / even n / odd n.
+// Residue classes of n.  The reference splits n by parity when b is a
+// quadratic non-residue mod p (e = 2) and filters with d-th power residues
+// (setup.cl:22-87).  Here both come from one character of larger order.  Let D
+// be the part of p-1 made of the primes up to 61, and chi(x) = x^((p-1)/D),
+// which maps onto the D-th roots of unity.  If k*b^n == -c then
+//      chi(b)^n = chi(-c) / chi(k),
+// so (1) a target is impossible unless chi(-c)/chi(k) lies in the subgroup
+// generated by chi(b), of order eo (the reference's filters are the cases
+// d | D of this), and (2) n mod e is fixed, for every divisor e of eo, by the
+// discrete logarithm of h = chi(b)^(eo/e) -- a table of e values.  e is the
+// largest divisor of eo up to 64.  Every n the reference finds satisfies both,
+// so the eliminated terms are the same, while each sequence's giant steps
+// shrink from L/Q to L/(e*Q) (e = 2 is the reference's parity case; at the
+// 2^50 p-range of the 100-sequence job e averages well above 2).
 // Primes dividing b or any k, and primes where no k survives, are skipped for
-// every sequence exactly as setup.cl:156-162,205-208 do.
+// every sequence as setup.cl:156-162,205-208 do.
 //
 // Kernel 1 (one thread per prime) does the per-prime scalars; kernel 2 (one
 // warp per prime, lanes over k) classifies the sequences and writes the
@@ -28,39 +36,57 @@
 
 namespace rs {
 
-__device__ __constant__ u32 c_DS[NDS] = {3, 4, 5, 7, 8, 9, 11, 13, 17, 19, 23, 29};
-
-// Legendre symbol (x/p) for x = 2^v2 * xodd, p an odd prime not dividing x,
-// by quadratic reciprocity: (xodd/p) = (p mod xodd / xodd) * (-1)^((xodd-1)/2*(p-1)/2).
-__device__ __forceinline__ int legendre_of(u64 xodd, u32 v2, u64 xrd, u64 p)
-{
-    int t = 1;
-    const u32 r8 = (u32)p & 7;
-    if ((v2 & 1) && (r8 == 3 || r8 == 5)) t = -t;      // (2/p)
-    if (xodd == 1) return t;
-    u64 a = mod_barrett(p, xodd, xrd);
-    if (a == 0) return 0;
-    if ((xodd & 3) == 3 && (p & 3) == 3) t = -t;
-    int j = (xodd >> 32) ? jacobi64(a, xodd) : jacobi32((u32)a, (u32)xodd);
-    return t * j;
-}
-
-// (p-1)/DS[j] for a compile-time j (division by a constant)
-__device__ __forceinline__ u64 pm1_div(u64 pm1, int j)
-{
-    switch (j) {
-    case 0: return pm1 / 3;   case 1: return pm1 >> 2;  case 2: return pm1 / 5;   case 3: return pm1 / 7;
-    case 4: return pm1 >> 3;  case 5: return pm1 / 9;   case 6: return pm1 / 11;  case 7: return pm1 / 13;
-    case 8: return pm1 / 17;  case 9: return pm1 / 19;  case 10: return pm1 / 23; default: return pm1 / 29;
-    }
-}
+constexpr u32 SPLIT_MAX = 64;        // largest split modulus e (6 bits of offset per target)
 
 struct PrimeAux {        // kernel 1 -> kernel 2 scalars
     u64 r2;              // R^2 mod p
-    u64 wr0, wr1;        // b^(nmin+e(Q-1)) * R^2 and b^(nmin+1+e(Q-1)) * R^2 (mod p)
-    u32 amask;           // active power-residue degrees (bit j <=> DS[j])
-    u32 pad_;
+    u64 wr0;             // b^(nmin + e(Q-1)) * R^2 (mod p)
+    u64 bm;              // Montgomery b
+    u64 xD;              // (p-1)/D: chi(x) = x^xD
+    u64 xe;              // eo/e
+    u64 h;               // Montgomery chi(b)^xe, of order e
+    u32 e;               // split modulus
+    u32 flags;           // AUX_* below
 };
+constexpr u32 AUX_NEG_EO = 1u;   // chi(-1)^eo = -1: for c = +1 the membership test wants z^eo == -1
+constexpr u32 AUX_NEG_XE = 2u;   // chi(-1)^xe = -1: for c = +1 the class search wants z1*h^r == -1
+
+// Moves every factor L of x into D (L a compile-time prime): applied for each
+// prime up to 61, it leaves D = the 61-smooth part of p-1 and x = (p-1)/D.
+template <u32 L>
+__device__ __forceinline__ void strip(u64 &x, u64 &D)
+{
+    while (x % L == 0) { x /= L; D *= L; }
+}
+
+// Order of g in the group of D-th roots of unity (D 61-smooth): remove the
+// prime factor L from eo while g^(eo/L) is still 1.
+template <u32 L>
+__device__ __forceinline__ void order_step(u64 &eo, u64 g, const Mont &M)
+{
+    while (eo % L == 0 && mpow(g, eo / L, M) == M.one) eo /= L;
+}
+
+// Largest divisor of eo that is at most SPLIT_MAX.
+__device__ __forceinline__ u32 split_modulus(u64 eo)
+{
+    u32 e = 1;
+#pragma unroll
+    for (u32 d = SPLIT_MAX; d > 1; --d)
+        if (e == 1 && eo % d == 0) e = d;
+    return e;
+}
+
+// b^e as an integer when it is at most 16 (baby steps by additions), else 0.
+__device__ __forceinline__ u32 small_power(u32 b, u32 e)
+{
+    u64 v = 1;
+    for (u32 i = 0; i < e; ++i) {
+        v *= b;
+        if (v > 16) return 0;
+    }
+    return (u32)v;
+}
 
 // Per-prime constants of prime p into record t.
 __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, u64 p, u32 t, u32 jb,
@@ -69,30 +95,39 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
 {
     PrimeHdr H;
     H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.job = jb;
-    H.Sh = 0; H.Sw = 0;
+    H.Mg = 0; H.pad_ = 0; H.Sh = 0; H.Sw = 0; H.ssw = 0;
     const Mont M = mont_init(p);
     const u32 b = job->base;
     const u64 bm = to_mont(b, M);
     if (bm == 0) { hdr[t] = H; return; }                 // p | b: no term is divisible by p
-    const int rg = legendre_of(job->bodd, job->bv2, job->brd, p);
-    const u32 e = (rg == -1) ? 2u : 1u;
-    const u64 s = (e == 2) ? mmul(bm, bm, p, M.q) : bm;
+    // D = 61-smooth part of p-1, xD = (p-1)/D
+    u64 xD = p - 1, D = 1;
+    strip<2>(xD, D);  strip<3>(xD, D);  strip<5>(xD, D);  strip<7>(xD, D);  strip<11>(xD, D);
+    strip<13>(xD, D); strip<17>(xD, D); strip<19>(xD, D); strip<23>(xD, D); strip<29>(xD, D);
+    strip<31>(xD, D); strip<37>(xD, D); strip<41>(xD, D); strip<43>(xD, D); strip<47>(xD, D);
+    strip<53>(xD, D); strip<59>(xD, D); strip<61>(xD, D);
+    const u64 gb = mpow(bm, xD, M);                       // chi(b), of order eo | D
+    u64 eo = D;
+    order_step<2>(eo, gb, M);  order_step<3>(eo, gb, M);  order_step<5>(eo, gb, M);  order_step<7>(eo, gb, M);
+    order_step<11>(eo, gb, M); order_step<13>(eo, gb, M); order_step<17>(eo, gb, M); order_step<19>(eo, gb, M);
+    order_step<23>(eo, gb, M); order_step<29>(eo, gb, M); order_step<31>(eo, gb, M); order_step<37>(eo, gb, M);
+    order_step<41>(eo, gb, M); order_step<43>(eo, gb, M); order_step<47>(eo, gb, M); order_step<53>(eo, gb, M);
+    order_step<59>(eo, gb, M); order_step<61>(eo, gb, M);
+    const u32 e = split_modulus(eo);
+    const u64 xe = eo / e;
+    const u64 s = mpow(bm, e, M);
     const u64 S = mpow(s, (u64)gm.q, M);
     const u64 W0 = mpow(bm, (u64)job->nmin + (u64)e * (gm.q - 1), M);
     PrimeAux X;
     X.r2 = M.r2;
     X.wr0 = mmul(W0, M.r2, p, M.q);
-    X.wr1 = mul_base(X.wr0, b, bm, M);
-    // d-th power residuosity of b (good_pr, setup.cl:11-48)
-    u32 am = 0;
-    const u64 pm1 = p - 1;
-#pragma unroll
-    for (int j = 0; j < NDS; ++j) {
-        u64 ex = pm1_div(pm1, j);
-        if (ex * c_DS[j] == pm1 && ex > 0 && mpow(bm, ex, M) == M.one) am |= 1u << j;
-    }
-    X.amask = am;
-    X.pad_ = 0;
+    X.bm = bm;
+    X.xD = xD;
+    X.xe = xe;
+    X.h = mpow(gb, xe, M);
+    X.e = e;
+    const bool chi_m1 = (xD & 1) != 0;                    // chi(-1) = (-1)^xD
+    X.flags = ((chi_m1 && (eo & 1)) ? AUX_NEG_EO : 0u) | ((chi_m1 && (xe & 1)) ? AUX_NEG_XE : 0u);
     // baby-step start tables: A[l] = s^(C*l), B[w] = s^(32*C*w)
     u64 *tb = tabs + (size_t)t * TABS;
     const u64 u = mpow(s, (u64)gm.c, M);
@@ -101,10 +136,17 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
     const u64 v = a;                                      // u^32
     a = M.one;
     for (int w = 0; w < 32; ++w) { tb[32 + w] = a; a = mmul(a, v, p, M.q); }
-    const u64 bb = (e == 2) ? (u64)b * b : (u64)b;
     H.p = p; H.q = M.q; H.one = M.one; H.s = s; H.S = S; H.e = e;
-    H.Sw = (p >> 63) ? 0 : shoup_const(from_mont(S, M), p);   // nonzero: from_mont(S) = s^Q != 0 mod p
-    H.smul = (bb <= 16) ? (u32)bb : 0u;
+    // Shoup quotients of s^Q (giant steps) and of s (baby steps) below 2^63;
+    // both residues are nonzero since p does not divide b
+    if (!(p >> 63)) {
+        H.Sw = shoup_const(from_mont(S, M), p);
+        H.ssw = shoup_const(from_mont(s, M), p);
+    }
+    H.smul = small_power(b, e);
+    // giant steps per target: ceil(ceil(L/e)/Q) cover every u of every offset
+    const u64 Le = ((u64)job->L + e - 1) / e;
+    H.Mg = (u32)((Le + gm.q - 1) / gm.q);
     hdr[t] = H;
     aux[t] = X;
 }
@@ -123,7 +165,7 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
                                                      const u32 *__restrict__ prefix, u32 nr, u32 rcap)
 {
     const u32 stride = gridDim.x * blockDim.x;
-    if (BATCH) {
+    if constexpr (BATCH) {
         const u32 total = prefix[nr];
         for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
             const u32 r = prefix_find(prefix, nr, i);
@@ -131,17 +173,19 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
             const u32 jb = ranges[r].job;
             setup_prime_one(jobs + jb, primes[rec], rec, jb, hdr, aux, tabs, geoms[jb]);
         }
-        return;
+    } else {
+        for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += stride)
+            setup_prime_one(jobs, primes[first + t], t, 0, hdr, aux, tabs, gm);
     }
-    for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += stride)
-        setup_prime_one(jobs, primes[first + t], t, 0, hdr, aux, tabs, gm);
 }
 
 // Sequence classes, targets and giant-step tables of record w (one warp).
+// tw: this warp's two tables of SPLIT_MAX entries in shared memory.
 __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 w, u32 lane, PrimeHdr *__restrict__ hdr,
                                             const PrimeAux *__restrict__ aux, u64 *__restrict__ tabs,
-                                            u64 *__restrict__ tgt, unsigned char *__restrict__ meta,
-                                            u64 *__restrict__ stats, const JobGeom &gm)
+                                            u64 *__restrict__ tgt, unsigned short *__restrict__ meta,
+                                            u64 *__restrict__ stats, u32 *__restrict__ err, const JobGeom &gm,
+                                            u64 *tw)
 {
     PrimeHdr H = hdr[w];
     if (H.p == 0) {
@@ -153,15 +197,24 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     M.p = H.p; M.q = H.q; M.one = H.one; M.r2 = X.r2;
     const u64 p = H.p;
     const u32 K = job->kcount;
-    const bool m1qr = ((p & 3) == 1);                     // (-1/p) = +1
+    const u32 e = X.e;
     const u64 mone = p - M.one;
+    // hinv[r] = h^(-r) = h^((e - r) mod e) and wt[r] = b^(nmin + e(Q-1) + r) * R^2, for r < e
+    u64 *hinv = tw, *wt = tw + SPLIT_MAX;
+    __syncwarp();                                          // the previous prime's readers are done
+    for (u32 r = lane; r < e; r += 32) {
+        hinv[r] = mpow(X.h, (u64)((e - r) % e), M);
+        wt[r] = mmul(X.wr0, mpow(X.bm, (u64)r, M), p, M.q);
+    }
+    __syncwarp();
+    const u32 nmod = job->nmin % e;
     u32 nk = 0;
-    bool divk = false;
+    bool divk = false, lost = false;
     for (u32 i0 = 0; i0 < K; i0 += 32) {
         const u32 i = i0 + lane;
         bool keep = false;
         u64 T = 0;
-        unsigned char mt = 0;
+        unsigned short mt = 0;
         if (i < K) {
             const u64 kv = job->k[i];
             const u64 kr = (kv < p) ? kv : kv % p;
@@ -169,27 +222,27 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
                 divk = true;
             } else {
                 const int ci = job->c[i];
-                int ra = legendre_of(job->kodd[i], job->kv2[i], job->krd[i], p);
-                if (ci == 1 && !m1qr) ra = -ra;           // (-c/p)(k/p) is the character of -c*k^-1
-                u32 off = 0;
-                bool ok;
-                if (H.e == 1) ok = (ra == 1);
-                else { ok = true; off = ((ra == 1) ? 0u : 1u) ^ (job->nmin & 1u); }   // n even <=> off == nmin mod 2
-                if (ok && X.amask) {
-                    const u64 km = to_mont(kr, M);
-#pragma unroll 1
-                    for (int j = 0; j < NDS; ++j) {
-                        if (!((X.amask >> j) & 1)) continue;
-                        const u64 ex = pm1_div(p - 1, j);
-                        const u64 want = (ci == 1 && (ex & 1)) ? mone : M.one;
-                        if (mpow(km, ex, M) != want) { ok = false; break; }
+                // z = chi(k); the target is possible iff (chi(-c)/z)^eo == 1, i.e.
+                // z1^e == chi(-c)^eo with z1 = z^xe; chi(-c) is 1 for c = -1
+                const u64 z1 = mpow(mpow(to_mont(kr, M), X.xD, M), X.xe, M);
+                const u64 want = (ci == 1 && (X.flags & AUX_NEG_EO)) ? mone : M.one;
+                if (mpow(z1, (u64)e, M) == want) {
+                    // n == r (mod e) where z1 * h^r == chi(-c)^xe
+                    const bool neg = (ci == 1) && (X.flags & AUX_NEG_XE);
+                    u32 r = e;
+                    for (u32 rr = 0; rr < e; ++rr) {
+                        const u64 hv = hinv[rr];
+                        if (z1 == (neg ? p - hv : hv)) { r = rr; break; }
                     }
-                }
-                if (ok) {
-                    T = mmul(kr, off ? X.wr1 : X.wr0, p, M.q);
-                    if (ci == 1) T = mneg(T, p);
-                    mt = (unsigned char)(i | (off << 7));
-                    keep = true;
+                    if (r < e) {
+                        const u32 off = (r + e - nmod) % e;
+                        T = mmul(kr, wt[off], p, M.q);
+                        if (ci == 1) T = mneg(T, p);
+                        mt = (unsigned short)(i | (off << 7));
+                        keep = true;
+                    } else {
+                        lost = true;                      // cannot happen: the class exists when the test passes
+                    }
                 }
             }
         }
@@ -201,6 +254,7 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
         }
         nk += __popc(km_);
     }
+    if (lost) atomicOr(err, ERR_SETUP_CLASS);
     divk = __any_sync(0xFFFFFFFFu, divk);
     if (divk || nk == 0) {
         if (lane == 0) {
@@ -210,7 +264,7 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
         return;
     }
     // giant-phase split: G chunks of Lc giant steps per target, numk*G <= tpb
-    const u32 Mg = (H.e == 2) ? gm.m2 : gm.m1;
+    const u32 Mg = H.Mg;
     u32 G = gm.tpb / nk;
     if (G < 1) G = 1;
     if (G > Mg) G = Mg;
@@ -240,60 +294,60 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
         hdr[w].Lc = Lc;
         hdr[w].Sh = sh;
         atomicAdd(&stats[ST_TARGETS], (u64)nk);
-        atomicAdd(&stats[H.e == 2 ? ST_PARITY : ST_FULL], 1ull);
+        atomicAdd(&stats[e >= 2 ? ST_PARITY : ST_FULL], 1ull);
     }
 }
 
 
 // Kernel 2: one warp per prime; lanes walk the sequences.  BATCH as kernel 1.
 template <bool BATCH>
-__global__ void __launch_bounds__(SETUP_TPB, 6) k_setup_k(const JobDev *__restrict__ jobs, PrimeHdr *__restrict__ hdr,
+__global__ void __launch_bounds__(SETUP_TPB, 4) k_setup_k(const JobDev *__restrict__ jobs, PrimeHdr *__restrict__ hdr,
                                                        const PrimeAux *__restrict__ aux, u32 count,
                                                        u64 *__restrict__ tabs, u64 *__restrict__ tgt,
-                                                       unsigned char *__restrict__ meta, u64 *__restrict__ stats,
-                                                       JobGeom gm, const JobGeom *__restrict__ geoms,
+                                                       unsigned short *__restrict__ meta, u64 *__restrict__ stats,
+                                                       u32 *__restrict__ err, JobGeom gm,
+                                                       const JobGeom *__restrict__ geoms,
                                                        const BatchRange *__restrict__ ranges,
                                                        const u32 *__restrict__ prefix, u32 nr, u32 rcap)
 {
+    __shared__ u64 s_tw[SETUP_TPB / 32][2 * SPLIT_MAX];   // per warp: class and target tables of its prime
     const u32 lane = threadIdx.x & 31;
     const u32 nwarps = gridDim.x * (SETUP_TPB / 32);
+    u64 *tw = s_tw[threadIdx.x >> 5];
     // w is uniform over the warp, so the warp-wide ballots of a prime stay whole
-    if (BATCH) {
+    if constexpr (BATCH) {
         const u32 total = prefix[nr];
         for (u32 i = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5; i < total; i += nwarps) {
             const u32 r = prefix_find(prefix, nr, i);
             const u32 rec = r * rcap + (i - prefix[r]);
             const u32 jb = ranges[r].job;
-            setup_k_one(jobs + jb, rec, lane, hdr, aux, tabs, tgt, meta, stats, geoms[jb]);
+            setup_k_one(jobs + jb, rec, lane, hdr, aux, tabs, tgt, meta, stats, err, geoms[jb], tw);
         }
-        return;
+    } else {
+        for (u32 w = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5; w < count; w += nwarps)
+            setup_k_one(jobs, w, lane, hdr, aux, tabs, tgt, meta, stats, err, gm, tw);
     }
-    for (u32 w = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5; w < count; w += nwarps)
-        setup_k_one(jobs, w, lane, hdr, aux, tabs, tgt, meta, stats, gm);
 }
 
 cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 count, PrimeHdr *hdr, void *aux, u64 *tabs,
-                         u64 *tgt, unsigned char *meta, u64 *stats, int geom, u32 L, cudaStream_t st)
+                         u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, int geom, cudaStream_t st)
 {
     if (count == 0) return cudaSuccess;
-    const BsgsGeom &g = BSGS_GEOMS[geom];
-    JobGeom gm;
-    gm.q = g.q; gm.c = g.c; gm.tpb = g.tpb; gm.pad_ = 0;
-    gm.m1 = (u32)(((u64)L + g.q - 1) / g.q);
-    gm.m2 = (u32)(((u64)L + 2ull * g.q - 1) / (2ull * g.q));
+    const JobGeom gm = job_geom(geom);
     k_setup_prime<false><<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, tabs, gm,
                                                               nullptr, nullptr, nullptr, 0, 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const u32 wpb = SETUP_TPB / 32;
     k_setup_k<false><<<(count + wpb - 1) / wpb, SETUP_TPB, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, tgt,
-                                                                   meta, stats, gm, nullptr, nullptr, nullptr, 0, 0);
+                                                                   meta, stats, err, gm, nullptr, nullptr, nullptr, 0,
+                                                                   0);
     return cudaGetLastError();
 }
 
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
                                u32 rcap, const u32 *prefix_p, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs,
-                               u64 *tgt, unsigned char *meta, u64 *stats, int sms, cudaStream_t st)
+                               u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, int sms, cudaStream_t st)
 {
     JobGeom gm{};
     // full-device grids; the kernels stride over the primes of every range
@@ -301,8 +355,8 @@ cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const B
                                                  prefix_p, nranges, rcap);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_setup_k<true><<<sms * 6, SETUP_TPB, 0, st>>>(jobs, hdr, (const PrimeAux *)aux, 0, tabs, tgt, meta, stats, gm,
-                                                   geoms, ranges, prefix_p, nranges, rcap);
+    k_setup_k<true><<<sms * 4, SETUP_TPB, 0, st>>>(jobs, hdr, (const PrimeAux *)aux, 0, tabs, tgt, meta, stats, err,
+                                                   gm, geoms, ranges, prefix_p, nranges, rcap);
     return cudaGetLastError();
 }
 
