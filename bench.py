@@ -320,13 +320,20 @@ def measure_config1(torch, rs, W, peak_g):
             "mulmods": {"gpu": mulmod_rates(c, gms / 1e3, peak_g)}}
 
 
-def measure_served(rs, W, serve, peak_g, seed=5, nunits=60, rate=8.0, width_log2=(22, 26)):
-    """Config-5 shape, scaled down: 16 config-2-style files, Poisson arrivals at `rate`
-    units/s, unit widths 2^22..2^26 (the full workload's are 2^30..2^36); latency
-    from arrival and from admission, and each unit's latency over its own run time
-    alone on the same server."""
+def measure_served(rs, W, serve, peak_g, seed=5, nunits=60, rate=8.0, width_log2=(22, 26), rho=None,
+                   primes_per_s=None, label=None):
+    """Config-5 shape: 16 config-2-style files, Poisson arrivals at `rate` units/s
+    (or, with rho, at the rate that loads the GPU to rho given its measured
+    primes_per_s), unit widths 2^width_log2 (the full workload's are 2^30..2^36);
+    latency from arrival and from admission, and each unit's latency over its own
+    run time alone on the same server."""
     import numpy as np
     files = [W.seqs_of(f) for f in W.config5_files(seed)]
+    if rho is not None:
+        # mean service time of a unit alone: its primes (width / ln p0) at the measured rate
+        probe = W.config5_units(seed, nunits, 1.0, len(files), width_log2)
+        mean_primes = sum((p1 - p0) / math.log(p0) for _, _, p0, p1 in probe) / len(probe)
+        rate = rho / (mean_primes / primes_per_s)
     raw = W.config5_units(seed, nunits, rate, len(files), width_log2)
     units = [serve.Unit(k, fi, p0, p1, t) for k, (t, fi, p0, p1) in enumerate(raw)]
     srv = serve.Server(files, max_units=48, range_slots=64)
@@ -345,8 +352,10 @@ def measure_served(rs, W, serve, peak_g, seed=5, nunits=60, rate=8.0, width_log2
             ratios.append((u.finished - u.arrival) / max(v.finished - v.admitted, 1e-6))
     finally:
         srv.close()
-    st.update({"workload": "config5 shape scaled down: %d units over 16 files, Poisson %.0f units/s, widths 2^%d..2^%d, "
-                           "starts 2^44..2^62" % (nunits, rate, width_log2[0], width_log2[1]),
+    st.update({"workload": label or ("config5 shape scaled down: %d units over 16 files, Poisson %.0f units/s, "
+                                     "widths 2^%d..2^%d, starts 2^44..2^62" % (nunits, rate, width_log2[0],
+                                                                               width_log2[1])),
+               "arrival_rate_per_s": rate,
                "latency_over_isolated_p50": float(np.percentile(ratios, 50)),
                "latency_over_isolated_p99": float(np.percentile(ratios, 99)),
                "latency_over_isolated_max": float(max(ratios)),
@@ -513,6 +522,10 @@ def main():
                                                             30, 32,
                                                             "config4 job (b=5, 20 seqs, k even < 2^40, p near 2^64)"),
                  "served": measure_served(rs, W, serve, peak)}
+        forms["served_stated"] = measure_served(
+            rs, W, serve, peak, seed=6, nunits=5, width_log2=(30, 31), rho=0.5, primes_per_s=value,
+            label="config5 units at the lower end of their stated widths: 5 units of 2^U{30..31} over 16 files, "
+                  "starts log-uniform in [2^44, 2^62], Poisson arrivals at the rate that loads the GPU to 0.5")
         rates = [float(x) for x in args.serve_rates.split(",") if x] if args.serve_rates else []
         if rates:
             forms["served_sweep"] = [measure_served(rs, W, serve, peak, rate=r) for r in rates]

@@ -11,9 +11,12 @@
 //   k_sieve_batch    segmented sieve, blockIdx.y = range
 //   k_mr_batch       Miller-Rabin over the survivors of every range at once
 //   k_setup_*<true>  per-prime set-up over the primes of every range at once
-//   per (geometry, product) group: prefix of the group's prime counts, then one
-//   persistent k_bsgs<..., true> over all primes of the group's ranges (each
-//   prime carries its job index and loads that job's arguments)
+//   k_batch_group_prefix  every (geometry, product) group's prefix sums of its
+//                    ranges' prime counts, in one launch
+//   per group, on its own branch (fork/join through events): one persistent
+//   k_bsgs<..., true> over all primes of the group's ranges (each prime carries
+//   its job index and loads that job's arguments); the branches overlap, so one
+//   group's last wave does not idle the device
 //   k_batch_account  primes tested per range, unfinished-range count
 //
 // so the host only waits once per round, to read the error word and whether
@@ -63,12 +66,7 @@ struct BJob {
     std::vector<u32> ranges;
 };
 
-struct Group {
-    int geom;
-    bool shoup;
-    u32 *d_prefix = nullptr;   // nr + 1 prefix sums of the group's prime counts
-    u32 *d_work = nullptr;     // work counter of the group's BSGS launch
-};
+constexpr int NGROUP = 2 * NGEOM;  // BSGS groups: g = 2*geometry + (1 for Shoup products below 2^63)
 
 __global__ void k_batch_account(const BatchRange *ranges, const u32 *ctrs, u32 rcap, u32 nranges, u64 *range_primes,
                                 u64 *stats, u32 *unfinished)
@@ -99,7 +97,10 @@ struct rs_batch {
     u32 *d_win = nullptr;
     u32 *d_prefix_c = nullptr, *d_prefix_p = nullptr;   // prefix sums over all ranges: survivors, primes
     u32 *h_win_pin = nullptr;
-    std::vector<Group> groups;
+    u32 *d_gprefix = nullptr;              // NGROUP x (nranges + 1) prefix sums of the groups' prime counts
+    u32 *d_gwork = nullptr;                // NGROUP work counters of the groups' BSGS launches
+    cudaStream_t side[NGROUP] = {};        // one branch per group: the groups' launches overlap
+    cudaEvent_t fork = nullptr, join[NGROUP] = {};
     // device tables
     u32 *d_sp = nullptr;
     u32 nsp = 0;
@@ -150,13 +151,15 @@ extern "C" void rs_batch_destroy(rs_batch *b)
     }
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->pool) cudaMemPoolDestroy(b->pool);
-    for (auto &g : b->groups) {
-        cudaFree(g.d_prefix);
-        cudaFree(g.d_work);
+    for (int g = 0; g < NGROUP; ++g) {
+        if (b->side[g]) cudaStreamDestroy(b->side[g]);
+        if (b->join[g]) cudaEventDestroy(b->join[g]);
     }
+    if (b->fork) cudaEventDestroy(b->fork);
     void *ptrs[] = {b->d_sp, b->d_jobs, b->d_geoms, b->d_args, b->d_fctrs, b->d_ranges, b->d_wins, b->d_ctrs,
                     b->d_range_primes, b->d_cands, b->d_primes, b->d_hdr, b->d_aux, b->d_tabs, b->d_tgt, b->d_meta,
-                    b->d_err, b->d_stats, b->d_unfinished, b->d_win, b->d_prefix_c, b->d_prefix_p};
+                    b->d_err, b->d_stats, b->d_unfinished, b->d_win, b->d_prefix_c, b->d_prefix_p,
+                    b->d_gprefix, b->d_gwork};
     for (void *p : ptrs) cudaFree(p);
     if (b->h_pin) cudaFreeHost(b->h_pin);
     if (b->h_win_pin) cudaFreeHost(b->h_win_pin);
@@ -245,16 +248,15 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         if (cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
             return fail(RS_ECUDA);
     }
-    for (int g = 0; g < NGEOM; ++g)
-        for (int m = 0; m < 2; ++m) {
-            Group G{g, m == 1, nullptr, nullptr};
-            if (!alloc((void **)&G.d_prefix, (R + 1) * 4) || !alloc((void **)&G.d_work, 4)) {
-                b->groups.push_back(G);
-                rs_set_error("cannot allocate the BSGS group tables");
-                return fail(RS_ENOMEM);
-            }
-            b->groups.push_back(G);
-        }
+    if (!alloc((void **)&b->d_gprefix, (size_t)NGROUP * (R + 1) * 4) || !alloc((void **)&b->d_gwork, NGROUP * 4)) {
+        rs_set_error("cannot allocate the BSGS group tables");
+        return fail(RS_ENOMEM);
+    }
+    if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess) return fail(RS_ECUDA);
+    for (int g = 0; g < NGROUP; ++g)
+        if (cudaStreamCreateWithFlags(&b->side[g], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->join[g], cudaEventDisableTiming) != cudaSuccess)
+            return fail(RS_ECUDA);
     *out = b;
     return RS_OK;
 }
@@ -486,11 +488,18 @@ static int batch_round(rs_batch *b)
     memset(&a, 0, sizeof a);
     a.stats = b->d_stats;
     a.err = b->d_err;
-    for (auto &g : b->groups) {
-        BCU(launch_batch_prefix(b->d_ranges, R, g.geom, g.shoup, b->d_ctrs, RCAP, g.d_prefix, st));
-        BCU(cudaMemsetAsync(g.d_work, 0, 4, st));
-        BCU(launch_bsgs_batch(a, b->d_args, b->d_hdr, b->d_tabs, b->d_tgt, b->d_meta, R, g.d_prefix, RCAP, g.d_work,
-                              g.shoup, g.geom, b->sms, st));
+    // the groups' prefix sums in one launch, then one persistent BSGS launch per
+    // group on its own branch (fork/join through events, so a captured round is
+    // a graph with parallel branches): one group's last wave overlaps the others
+    BCU(launch_batch_group_prefix(b->d_ranges, R, b->d_ctrs, RCAP, b->d_gprefix, b->d_gwork, st));
+    BCU(cudaEventRecord(b->fork, st));
+    for (int g = 0; g < NGROUP; ++g) {
+        BCU(cudaStreamWaitEvent(b->side[g], b->fork, 0));
+        BCU(launch_bsgs_batch(a, b->d_args, b->d_hdr, b->d_tabs, b->d_tgt, b->d_meta, R,
+                              b->d_gprefix + (size_t)g * (R + 1), RCAP, b->d_gwork + g, (g & 1) != 0, g >> 1, b->sms,
+                              b->side[g]));
+        BCU(cudaEventRecord(b->join[g], b->side[g]));
+        BCU(cudaStreamWaitEvent(st, b->join[g], 0));
     }
     k_batch_account<<<(R + 127) / 128, 128, 0, st>>>(b->d_ranges, b->d_ctrs, RCAP, R, b->d_range_primes, b->d_stats,
                                                      b->d_unfinished);

@@ -2,19 +2,21 @@
 //
 // Replaces the reference's giantfull/giantparity kernels (kernels/giant.cl:77-323).
 // For one prime p with per-prime record (see setup.cu):
-//   baby phase   y_j = s^j for j in [0,Q), Q = TPB*C: thread t computes
-//                y_{tC..tC+C-1} from its start A[t%32]*B[t/32] with C-1 cheap
-//                steps (additions when b^e <= 16), checks y_j == 1 to detect
-//                ord(s) < Q (giant.cl:123-134), then inserts j < ord into a
-//                shared-memory hash table.
+//   baby phase   y_j = s^j for j in [0,Q'), Q' = TPB*cp with cp = C, C/2 or
+//                C/4 chosen per prime by the set-up: thread t computes
+//                y_{t*cp..t*cp+cp-1} from its start A[t%32]*B[t/32] with cheap
+//                steps (doublings when b^e is 2 or 4, else one modular
+//                product), checks y_j == 1 to detect ord(s) < Q'
+//                (giant.cl:123-134), then inserts j < ord into a shared-memory
+//                hash table.
 //   giant phase  gamma = T_i * S^q for q in [0,Mg): thread (i,g) walks q in
 //                [g*Lc, (g+1)*Lc) from T_i * S^(g*Lc) as two interleaved
 //                chains, one modular product (Shoup's for p < 2^63, else
 //                Montgomery) and one table probe per step (giant.cl:170-192).  A match
-//                s^j == gamma gives n = nmin + off_i + e*((q+1)*Q - 1 - j),
+//                s^j == gamma gives n = nmin + off_i + e*((q+1)*Q' - 1 - j),
 //                where s = b^e and off_i is target i's class of n mod e
 //                (setup.cu; e = 2 is the reference's parity split).
-//   small order  ord(s) < Q: each target is looked up once and every n in
+//   small order  ord(s) < Q': each target is looked up once and every n in
 //                range with the same residue mod e*ord is claimed (giant.cl:146-168).
 //   claims       atomicAnd on the term's bitmap bit; the first claimer appends
 //                {p, n, seq} to the factor buffer (giant.cl:21-39,158-162).
@@ -177,13 +179,15 @@ constexpr u32 WAIT_BOUND = 1u << 24;   // default try_wait rounds before a copy 
 // overflowed buckets, small orders and claims run in __noinline__ functions
 // that take a few scalars and find everything else here.
 struct PrimeCtx {
-    u64 p, q, s;         // the prime, -p^-1 mod 2^64, Montgomery b^e
-    u32 smul, e;         // baby-step multiplier when additions suffice; 1 or 2
+    u64 p, q, s;         // the prime, p^-1 mod 2^64, Montgomery b^e
+    u32 smul, e;         // baby-step multiplier when additions suffice; split modulus
+    u32 cp, qp;          // baby steps per thread and per prime (qp = TPB * cp)
 };
 extern __shared__ __align__(128) unsigned char smem_raw[];
 __shared__ BsgsArgs s_args;
 __shared__ PrimeCtx s_ctx;
 __shared__ unsigned long long s_cands, s_dups, s_facs;   // per-CTA totals
+__shared__ unsigned long long s_baby, s_giant, s_small;  // per-CTA totals kept by thread 0
 __shared__ u32 s_nsol, s_sol_i[KMAX], s_sol_u0[KMAX];   // small-order solutions
 
 // Dynamic shared memory: fingerprints | indices | counts | start values | giant
@@ -228,22 +232,21 @@ __device__ __forceinline__ void claim(u64 p, u32 seq, u32 n)
 }
 
 // exact check of a fingerprint match: y_j == val ?  (y_j from its thread's start)
-template <int C>
-__device__ __forceinline__ bool verify(const u64 *s_start, u32 j, u64 val, u32 Q)
+__device__ __forceinline__ bool verify(const u64 *s_start, u32 j, u64 val)
 {
-    if (j >= Q) return false;
     const PrimeCtx c = s_ctx;
-    u64 y = s_start[j / C];
-    for (u32 r = j % C; r; --r) y = baby_step(y, c.smul, c.s, c.p, c.q);
+    if (j >= c.qp) return false;
+    u64 y = s_start[j / c.cp];
+    for (u32 r = j % c.cp; r; --r) y = baby_step(y, c.smul, c.s, c.p, c.q);
     return y == val;
 }
 
 // Giant-step match or overflowed bucket: check every matching slot of the
-// chain starting at bucket b exactly and claim n = nmin + off + e*((q+1)Q-1-j).
+// chain starting at bucket b exactly and claim n = nmin + off + e*((q+1)Q'-1-j).
 template <int TPB, int C, int NB>
 __device__ __noinline__ void giant_slow(u64 gamma, u32 b, u32 fp, u32 qq, u32 meta)
 {
-    constexpr u32 Q = TPB * C;
+    const u32 Q = s_ctx.qp;
     const Table T = Smem<TPB, NB>::table();
     const u64 *st = Smem<TPB, NB>::start();
     for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
@@ -253,7 +256,7 @@ __device__ __noinline__ void giant_slow(u64 gamma, u32 b, u32 fp, u32 qq, u32 me
             if (slot_fp(bv, k) != fp) continue;
             atomicAdd(&s_cands, 1ull);
             const u32 j = T.jt[8 * b + k];
-            if (!verify<C>(st, j, gamma, Q)) continue;
+            if (!verify(st, j, gamma)) continue;
             const u64 u = (u64)(qq + 1) * Q - 1 - j;
             const u64 n = (u64)s_args.nmin + (meta >> 7) + (u64)s_ctx.e * u;
             if (n <= s_args.nmax) claim(s_ctx.p, meta & 0x7Fu, (u32)n);
@@ -305,7 +308,7 @@ __device__ __forceinline__ void clear_table(const Table &T, u32 nb)
     for (u32 i = threadIdx.x; i < nb / 8; i += blockDim.x) reinterpret_cast<uint4 *>(T.cnt)[i] = make_uint4(0u, 0u, 0u, 0u);
 }
 
-// ord(s) < Q: rebuild the table from the distinct values j < ord (the
+// ord(s) < Q': rebuild the table from the distinct values j < ord (the
 // speculative one may hold repeats).  Called by the whole CTA.
 template <int TPB, int C, int NB>
 __device__ __noinline__ void rebuild_table(u32 order)
@@ -317,8 +320,8 @@ __device__ __noinline__ void rebuild_table(u32 order)
     __syncthreads();
     u64 y = st[threadIdx.x];
     u32 pend = 0;
-    for (int i = 0; i < C; ++i) {
-        const u32 j = threadIdx.x * C + i;
+    for (u32 i = 0; i < c.cp; ++i) {
+        const u32 j = threadIdx.x * c.cp + i;
         if (j < order) {
             u32 b, fpv;
             tab_hash<NB>(y, b, fpv);
@@ -332,12 +335,12 @@ __device__ __noinline__ void rebuild_table(u32 order)
     __syncthreads();
 }
 
-// ord(s) < Q: each target is looked up once; every n in range with the same
+// ord(s) < Q': each target is looked up once; every n in range with the same
 // residue mod e*ord is claimed (giant.cl:146-168).  Called by the whole CTA.
 template <int TPB, int C, int NB>
 __device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
 {
-    constexpr u32 Q = TPB * C;
+    const u32 Q = s_ctx.qp;
     const Table T = Smem<TPB, NB>::table();
     const u64 *st = Smem<TPB, NB>::start();
     const u32 tid = threadIdx.x;
@@ -351,7 +354,7 @@ __device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
                 if (slot_fp(bv, k) != fp) continue;
                 atomicAdd(&s_cands, 1ull);
                 const u32 j = T.jt[8 * b + k];
-                if (j >= order || !verify<C>(st, j, Tv, Q)) continue;
+                if (j >= order || !verify(st, j, Tv)) continue;
                 const u32 ks = atomicAdd(&s_nsol, 1u);
                 s_sol_i[ks] = tid;
                 s_sol_u0[ks] = (Q - 1 - j) % order;
@@ -403,7 +406,9 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
     };
     constexpr u32 Q = TPB * C;
     static_assert(Q <= 65536, "baby indices are stored in 16 bits");
-    constexpr int IB = 8;                                         // values inserted per batch
+    static_assert(NB <= 65536, "bucket indices are packed into 16 bits");
+    constexpr int IBMAX = (C < 8) ? C : 8;                        // values inserted per round
+    static_assert(C % IBMAX == 0 && IBMAX % 4 == 0, "cp in {C, C/2, C/4} must split into rounds");
     const Table T = Smem<TPB, NB>::table();
     u64 *s_start = Smem<TPB, NB>::start();
     u64 *s_Z = Smem<TPB, NB>::zs();
@@ -422,7 +427,6 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         bulk_load(r->tgt, tgt + (size_t)idx * KSTRIDE, KSTRIDE * 8, &s_bar[buf]);
         bulk_load(r->meta, meta + (size_t)idx * KSTRIDE, KSTRIDE * 2, &s_bar[buf]);
     };
-    u64 st_baby = 0, st_giant = 0, st_small = 0;                  // thread 0's tallies
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
@@ -433,6 +437,9 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         s_cands = 0;
         s_dups = 0;
         s_facs = 0;
+        s_baby = 0;
+        s_giant = 0;
+        s_small = 0;
         const u32 i0 = slot_of(atomicAdd(work_ctr, 1u));
         s_idx[0] = i0;
         if (i0 != NONE) fetch(0, i0);
@@ -461,6 +468,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         const bool live = (R.hdr.p != 0);
         const u64 p = R.hdr.p, q = R.hdr.q, s = R.hdr.s;
         const u32 e = R.hdr.e, smul = R.hdr.smul;
+        const u32 cp = R.hdr.cp;                                  // baby steps per thread for this prime
         // claim the next prime; the result is consumed after the table clear,
         // so this warp keeps issuing while the atomic is in flight
         u32 nxt = 0;
@@ -469,6 +477,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             s_nsol = 0;
             s_spill = 0;
             s_ctx.p = p; s_ctx.q = q; s_ctx.s = s; s_ctx.smul = smul; s_ctx.e = e;
+            s_ctx.cp = cp; s_ctx.qp = TPB * cp;
             if (BATCH) s_args = job_args[R.hdr.job];
             nxt = slot_of(atomicAdd(work_ctr, 1u));
         }
@@ -484,11 +493,11 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         }
         if (live) {
             if (tid < R.hdr.G) s_Z[tid] = mmul(R.tabs[64 + (tid & 31)], R.tabs[96 + (tid >> 5)], p, q);
-            // ---- baby steps y_j = s^j, inserted as they are produced ----
-            // Speculative: ord(s) < Q is only known after the barrier; then the
+            // ---- baby steps y_j = s^j, j < Q' = TPB*cp, inserted as they are produced ----
+            // Speculative: ord(s) < Q' is only known after the barrier; then the
             // table (which may hold repeats) is rebuilt from j < ord.
             const u64 one = R.hdr.one;
-            u64 x = mmul(R.tabs[tid & 31], R.tabs[32 + (tid >> 5)], p, q);   // s^(C*tid)
+            u64 x = mmul(R.tabs[tid & 31], R.tabs[32 + (tid >> 5)], p, q);   // s^(cp*tid)
             s_start[tid] = x;
             u32 spill = 0;
             // The step kind is uniform per prime (b^e = 2, 4 or other) and is
@@ -498,35 +507,46 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             // (the same residues as the Montgomery product verify() uses).
             u32 minj = 0xFFFFFFFFu;
             const u64 ssw = R.hdr.ssw;
-            const u64 sp = (MODE == 1 && smul != 2 && smul != 4) ? from_mont(s, Mont{p, q, 0, 0}) : 0;
-            auto babies = [&](auto kind) {
+            const u64 sp = R.hdr.sp;
+            // cp is C, C/2 or C/4: IB values are hashed and stepped, then
+            // inserted, per round (IB = 8, or cp when it is smaller)
+            auto babies = [&](auto kind, auto ibc) {
                 constexpr int K = decltype(kind)::value;          // 2, 4: doublings; 1: Shoup; 0: baby_step
-#pragma unroll
-                for (int h0 = 0; h0 < C; h0 += IB) {
-                    u32 bk[IB], fp[IB], old[IB];
+                constexpr int IB = decltype(ibc)::value;
+#pragma unroll 1
+                for (u32 h0 = 0; h0 < cp; h0 += IB) {
+                    u32 bf[IB], old[IB];                          // bucket << 16 | fingerprint; claimed slot
 #pragma unroll
                     for (int i = 0; i < IB; ++i) {
-                        const u32 j = tid * C + h0 + i;
+                        const u32 j = tid * cp + h0 + i;
                         if (j != 0 && x == one && minj == 0xFFFFFFFFu) minj = j;
-                        tab_hash<NB>(x, bk[i], fp[i]);
+                        u32 bk, fp;
+                        tab_hash<NB>(x, bk, fp);
+                        bf[i] = (bk << 16) | fp;
                         if (K == 0) x = baby_step(x, smul, s, p, q);
                         else if (K == 1) x = shoup_mul(x, sp, ssw, p);
                         else if (MODE == 1) { x = dbl63(x, p); if (K == 4) x = dbl63(x, p); }
                         else { x = madd(x, x, p); if (K == 4) x = madd(x, x, p); }
                     }
 #pragma unroll
-                    for (int i = 0; i < IB; ++i) old[i] = tab_claim(T, bk[i]);
+                    for (int i = 0; i < IB; ++i) old[i] = tab_claim(T, bf[i] >> 16);
 #pragma unroll
                     for (int i = 0; i < IB; ++i) {
-                        const u32 j = tid * C + h0 + i;
-                        if (!tab_fill(T, bk[i], old[i], fp[i], j)) spill |= insert_walk<NB>(bk[i], fp[i], j, BSGS_SPEC_PROBE);
+                        const u32 j = tid * cp + h0 + i;
+                        const u32 bk = bf[i] >> 16, fp = bf[i] & 0xFFFFu;
+                        if (!tab_fill(T, bk, old[i], fp, j)) spill |= insert_walk<NB>(bk, fp, j, BSGS_SPEC_PROBE);
                     }
                 }
             };
-            if (smul == 2) babies(std::integral_constant<int, 2>{});
-            else if (smul == 4) babies(std::integral_constant<int, 4>{});
-            else if (MODE == 1) babies(std::integral_constant<int, 1>{});
-            else babies(std::integral_constant<int, 0>{});
+            auto babies_cp = [&](auto kind) {
+                if (cp >= IBMAX) babies(kind, std::integral_constant<int, IBMAX>{});
+                else if (cp >= IBMAX / 2) babies(kind, std::integral_constant<int, IBMAX / 2>{});
+                else babies(kind, std::integral_constant<int, IBMAX / 4>{});
+            };
+            if (smul == 2) babies_cp(std::integral_constant<int, 2>{});
+            else if (smul == 4) babies_cp(std::integral_constant<int, 4>{});
+            else if constexpr (MODE == 1) babies_cp(std::integral_constant<int, 1>{});
+            else babies_cp(std::integral_constant<int, 0>{});
             if (minj != 0xFFFFFFFFu) atomicMin(&s_order, minj);
             if (spill) s_spill = 1;
         }
@@ -534,7 +554,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         const u32 order = s_order;
         const u32 Mg = R.hdr.Mg;
         if (live) {
-            if (order < Q) rebuild_table<TPB, C, NB>(order);
+            if (order != 0xFFFFFFFFu) rebuild_table<TPB, C, NB>(order);
             else if (tid == 0 && s_spill) atomicOr(a.err, ERR_HASH_OVERFLOW);
 
             if (order == 0xFFFFFFFFu) {
@@ -542,11 +562,10 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                 // chain A walks q in [q0, q0+h), chain B q in [q0+h, q1), h = Lc/2;
                 // B starts from A's start times S^h (Sh), so the two products of
                 // a step are independent and overlap in the pipeline.  Below
-                // 2^63 the step is Shoup's product by the fixed s^Q (Sw is its
+                // 2^63 the step is Shoup's product by the fixed s^Q' (Sw is its
                 // quotient constant), else the Montgomery product by S.
                 const u32 numk = R.hdr.numk, G = R.hdr.G, Lc = R.hdr.Lc;
-                const u64 S = R.hdr.S, Sw = R.hdr.Sw;
-                const u64 Sp = from_mont(S, Mont{p, q, 0, 0});
+                const u64 S = R.hdr.S, Sw = R.hdr.Sw, Sp = R.hdr.Sp;
                 if (tid < numk * G) {
                     const u32 i = tid / G, g = tid - i * G;
                     const u32 q0 = g * Lc;
@@ -579,17 +598,17 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                 small_order_search<TPB, C, NB>(&R, order);
             }
             if (tid == 0) {
-                st_baby += min(order, Q);
-                if (order == 0xFFFFFFFFu) st_giant += (u64)R.hdr.numk * Mg;
-                else st_small += 1;
+                s_baby += min(order, TPB * cp);
+                if (order == 0xFFFFFFFFu) s_giant += (u64)R.hdr.numk * Mg;
+                else s_small += 1;
             }
         }
         __syncthreads();
     }
     if (tid == 0) {
-        atomicAdd(&a.stats[ST_BABY], st_baby);
-        atomicAdd(&a.stats[ST_GIANT], st_giant);
-        atomicAdd(&a.stats[ST_SMALLORDER], st_small);
+        atomicAdd(&a.stats[ST_BABY], s_baby);
+        atomicAdd(&a.stats[ST_GIANT], s_giant);
+        atomicAdd(&a.stats[ST_SMALLORDER], s_small);
         atomicAdd(&a.stats[ST_CANDIDATES], s_cands);
         atomicAdd(&a.stats[ST_DUPS], s_dups);
         atomicAdd(&a.stats[ST_FACTORS], s_facs);
@@ -724,10 +743,47 @@ __global__ void __launch_bounds__(256) k_batch_prefix(const BatchRange *ranges, 
     }
 }
 
-cudaError_t launch_batch_prefix(const BatchRange *ranges, u32 nr, int geom, bool shoup, const u32 *ctrs, u32 rcap,
-                                u32 *prefix, cudaStream_t st)
+// Every BSGS group's prefix sums in one launch: block g computes those of
+// group g = 2*geometry + (1 for Shoup products) into prefix + g*(nr+1) and
+// clears the group's work counter.
+__global__ void __launch_bounds__(256) k_batch_group_prefix(const BatchRange *ranges, u32 nr, const u32 *ctrs,
+                                                            u32 rcap, u32 *prefix, u32 *work)
 {
-    k_batch_prefix<<<1, 256, 0, st>>>(ranges, nr, geom, shoup ? 1 : 0, ctrs, rcap, prefix, 1);
+    __shared__ u32 part[256];
+    const u32 g = blockIdx.x;
+    const int geom = (int)(g >> 1), shoup = (int)(g & 1);
+    u32 *pf = prefix + (size_t)g * (nr + 1);
+    const u32 t = threadIdx.x;
+    if (t == 0) work[g] = 0;
+    const u32 per = (nr + 255) / 256;
+    const u32 k0 = t * per, k1 = min(k0 + per, nr);
+    auto cnt = [&](u32 k) -> u32 {
+        const BatchRange R = ranges[k];
+        const bool in = R.active && R.geom == geom && R.shoup == shoup;
+        return in ? min(ctrs[k * BR_CTRS + 1], rcap) : 0u;
+    };
+    u32 sum = 0;
+    for (u32 k = k0; k < k1; ++k) sum += cnt(k);
+    part[t] = sum;
+    __syncthreads();
+    for (u32 o = 1; o < 256; o <<= 1) {
+        const u32 v = (t >= o) ? part[t - o] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    u32 acc = part[t] - sum;
+    if (t == 0) pf[0] = 0;
+    for (u32 k = k0; k < k1; ++k) {
+        acc += cnt(k);
+        pf[k + 1] = acc;
+    }
+}
+
+cudaError_t launch_batch_group_prefix(const BatchRange *ranges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix,
+                                      u32 *work, cudaStream_t st)
+{
+    k_batch_group_prefix<<<2 * NGEOM, 256, 0, st>>>(ranges, nr, ctrs, rcap, prefix, work);
     return cudaGetLastError();
 }
 

@@ -40,17 +40,10 @@ RS_DEV u64 shoup_mul(u64 x, u64 w, u64 wp, u64 p)
     return (r >= p) ? r - p : r;
 }
 
-// floor(w * 2^64 / p) for w < p < 2^63: 64 steps of binary long division.
-RS_DEV u64 shoup_const(u64 w, u64 p)
-{
-    u64 r = w, qt = 0;
-    for (int i = 0; i < 64; ++i) {
-        r <<= 1;                  // r < p < 2^63, so 2r does not wrap
-        qt <<= 1;
-        if (r >= p) { r -= p; qt |= 1; }
-    }
-    return qt;
-}
+// Shoup's quotient floor(w * 2^64 / p) of the plain value w < p < 2^63, from
+// its Montgomery form wm = w * 2^64 mod p: w * 2^64 = wp * p + wm, so
+// wp * p == -wm (mod 2^64) and wp = -wm * p^-1 mod 2^64 (q = p^-1 mod 2^64).
+RS_DEV u64 shoup_of_mont(u64 wm, u64 q) { return (0 - wm) * q; }
 
 // a + b mod p for a, b in [0,p); correct for p up to 2^64-1 (wrapping add).
 RS_DEV u64 madd(u64 a, u64 b, u64 p)

@@ -110,24 +110,25 @@ struct JobDev {
     u32 *bitmap;         // kcount * words
 };
 
-struct PrimeHdr {        // 96 bytes (a 16-byte multiple: copied by TMA bulk copies)
+struct PrimeHdr {        // 112 bytes (a 16-byte multiple: copied by TMA bulk copies)
     u64 p;               // 0 = skipped
     u64 q;               // p^-1 mod 2^64
     u64 one;             // 2^64 mod p
     u64 s;               // Montgomery b^e, e = the split modulus (n runs over one class mod e per target)
-    u64 S;               // Montgomery s^Q
+    u64 S;               // Montgomery s^Q' (Q' = this prime's baby-step count)
     u32 numk;            // surviving targets
     u32 e;               // split modulus, 1..64
     u32 G, Lc;           // giant phase: G chunks of Lc giant steps
     u32 smul;            // b^e as an integer when the baby step uses additions, else 0
     u32 job;             // job index within a batch (0 for a single job)
-    u32 Mg;              // giant steps per target: ceil(ceil(L/e)/Q)
-    u32 pad_;
+    u32 Mg;              // giant steps per target: ceil(ceil(L/e)/Q'), Q' = TPB*cp
+    u32 cp;              // baby steps per thread for this prime (C, C/2 or C/4 of the launch's geometry)
     u64 Sh;              // Montgomery S^(Lc/2): start of a thread's second giant chain
-    u64 Sw;              // floor(Sp*2^64/p), Sp = s^Q mod p (plain), for Shoup giant steps; 0 when p >= 2^63
+    u64 Sw;              // floor(Sp*2^64/p), Sp = s^Q' mod p (plain), for Shoup giant steps; 0 when p >= 2^63
     u64 ssw;             // floor(sp*2^64/p), sp = s mod p (plain), for Shoup baby steps; 0 when p >= 2^63
+    u64 sp, Sp;          // s and s^Q' as plain residues, the Shoup multipliers (0 when p >= 2^63)
 };
-static_assert(sizeof(PrimeHdr) == 96, "PrimeHdr is copied in 16-byte units");
+static_assert(sizeof(PrimeHdr) == 112, "PrimeHdr is copied in 16-byte units");
 
 struct FactorRec {       // one claimed term: p | k[seq]*b^n + c[seq]
     u64 p;
@@ -220,10 +221,11 @@ cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
                                u32 rcap, const u32 *prefix_p, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs,
                                u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, int sms, cudaStream_t st);
-// one BSGS launch per (geometry, mode) group over range slots [0, nr): prefix
-// (nr+1 entries) counts the primes of the active slots of that group only
-cudaError_t launch_batch_prefix(const BatchRange *ranges, u32 nr, int geom, bool shoup, const u32 *ctrs, u32 rcap,
-                                u32 *prefix, cudaStream_t st);
+// one BSGS launch per (geometry, mode) group g = 2*geometry + shoup over range
+// slots [0, nr): prefix + g*(nr+1) (nr+1 entries) counts the primes of the
+// active slots of that group only; work[g] is cleared
+cudaError_t launch_batch_group_prefix(const BatchRange *ranges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix,
+                                      u32 *work, cudaStream_t st);
 // prefix over every active range of counter `which` (0: survivors, 1: primes), each capped at cap
 cudaError_t launch_batch_prefix_all(const BatchRange *ranges, u32 nr, int which, u32 cap, const u32 *ctrs,
                                     u32 *prefix, cudaStream_t st);

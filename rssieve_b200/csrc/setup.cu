@@ -29,8 +29,13 @@
 // every sequence as setup.cl:156-162,205-208 do.
 //
 // Kernel 1 (one thread per prime) does the per-prime scalars; kernel 2 (one
-// warp per prime, lanes over k) classifies the sequences and writes the
-// compacted targets and the giant-step start tables.
+// warp per prime, lanes over k) classifies the sequences, chooses the prime's
+// baby-step count Q' (the launch's Q, Q/2 or Q/4: fewer baby steps when the
+// split modulus leaves few giant steps) and writes the compacted targets;
+// kernel 3 (one thread per prime) writes the giant-step split and the baby-
+// and giant-step start tables.  Per-prime work that is the same for every
+// sequence runs one prime per thread, where it costs 1/32 of the issue slots
+// it would take in the warp-per-prime kernel.
 #include "mont.cuh"
 #include "rs_internal.h"
 
@@ -38,13 +43,20 @@ namespace rs {
 
 constexpr u32 SPLIT_MAX = 64;        // largest split modulus e (6 bits of offset per target)
 
+// mpow out of line, for the per-prime powers off the kernels' main path: one
+// copy of the loop keeps the kernels small enough for the instruction cache.
+__device__ __noinline__ u64 mpow_call(u64 x, u64 e, Mont M) { return mpow(x, e, M); }
+
+constexpr int NCP = 3;            // baby steps per thread: C, C/2 or C/4 (index k: C >> k)
+
 struct PrimeAux {        // kernel 1 -> kernel 2 scalars
     u64 r2;              // R^2 mod p
-    u64 wr0;             // b^(nmin + e(Q-1)) * R^2 (mod p)
     u64 bm;              // Montgomery b
     u64 xD;              // (p-1)/D: chi(x) = x^xD
     u64 xe;              // eo/e
     u64 h;               // Montgomery chi(b)^xe, of order e
+    u64 wr0[NCP];        // per baby-step count Q'_k = tpb*(C >> k): b^(nmin + e(Q'_k - 1)) * R^2 (mod p)
+    u64 S[NCP];          //   and Montgomery s^Q'_k
     u32 e;               // split modulus
     u32 flags;           // AUX_* below
 };
@@ -64,7 +76,7 @@ __device__ __forceinline__ void strip(u64 &x, u64 &D)
 template <u32 L>
 __device__ __forceinline__ void order_step(u64 &eo, u64 g, const Mont &M)
 {
-    while (eo % L == 0 && mpow(g, eo / L, M) == M.one) eo /= L;
+    while (eo % L == 0 && mpow_call(g, eo / L, M) == M.one) eo /= L;
 }
 
 // Largest divisor of eo that is at most SPLIT_MAX.
@@ -88,14 +100,15 @@ __device__ __forceinline__ u32 small_power(u32 b, u32 e)
     return (u32)v;
 }
 
-// Per-prime constants of prime p into record t.
+// Per-prime constants of prime p into record t, with the powers that depend
+// on the baby-step count for each of the counts kernel 2 chooses from.
 __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, u64 p, u32 t, u32 jb,
                                                 PrimeHdr *__restrict__ hdr, PrimeAux *__restrict__ aux,
-                                                u64 *__restrict__ tabs, const JobGeom &gm)
+                                                const JobGeom &gm)
 {
     PrimeHdr H;
     H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.job = jb;
-    H.Mg = 0; H.pad_ = 0; H.Sh = 0; H.Sw = 0; H.ssw = 0;
+    H.Mg = 0; H.cp = 0; H.Sh = 0; H.Sw = 0; H.ssw = 0; H.sp = 0; H.Sp = 0;
     const Mont M = mont_init(p);
     const u32 b = job->base;
     const u64 bm = to_mont(b, M);
@@ -115,51 +128,48 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
     order_step<59>(eo, gb, M); order_step<61>(eo, gb, M);
     const u32 e = split_modulus(eo);
     const u64 xe = eo / e;
-    const u64 s = mpow(bm, e, M);
-    const u64 S = mpow(s, (u64)gm.q, M);
-    const u64 W0 = mpow(bm, (u64)job->nmin + (u64)e * (gm.q - 1), M);
+    const u64 s = mpow_call(bm, e, M);
     PrimeAux X;
     X.r2 = M.r2;
-    X.wr0 = mmul(W0, M.r2, p, M.q);
     X.bm = bm;
     X.xD = xD;
     X.xe = xe;
-    X.h = mpow(gb, xe, M);
+    X.h = mpow_call(gb, xe, M);
     X.e = e;
     const bool chi_m1 = (xD & 1) != 0;                    // chi(-1) = (-1)^xD
     X.flags = ((chi_m1 && (eo & 1)) ? AUX_NEG_EO : 0u) | ((chi_m1 && (xe & 1)) ? AUX_NEG_XE : 0u);
-    // baby-step start tables: A[l] = s^(C*l), B[w] = s^(32*C*w)
-    u64 *tb = tabs + (size_t)t * TABS;
-    const u64 u = mpow(s, (u64)gm.c, M);
-    u64 a = M.one;
-    for (int l = 0; l < 32; ++l) { tb[l] = a; a = mmul(a, u, p, M.q); }
-    const u64 v = a;                                      // u^32
-    a = M.one;
-    for (int w = 0; w < 32; ++w) { tb[32 + w] = a; a = mmul(a, v, p, M.q); }
-    H.p = p; H.q = M.q; H.one = M.one; H.s = s; H.S = S; H.e = e;
-    // Shoup quotients of s^Q (giant steps) and of s (baby steps) below 2^63;
-    // both residues are nonzero since p does not divide b
-    if (!(p >> 63)) {
-        H.Sw = shoup_const(from_mont(S, M), p);
-        H.ssw = shoup_const(from_mont(s, M), p);
+    // Q'_k = 2^(m+2-k), m = log2(Q/4): s^(Q'-1) by t <- t^2 * s from s^(2^m - 1)
+    {
+        const u64 bn = mpow_call(bm, (u64)job->nmin, M);
+        const int m = __ffs((int)(gm.q >> 2)) - 1;
+        u64 tq = M.one;
+        for (int i = 0; i < m; ++i) tq = mmul(mmul(tq, tq, p, M.q), s, p, M.q);
+#pragma unroll
+        for (int k = NCP - 1; k >= 0; --k) {              // k = NCP-1: Q/4, then Q/2, Q
+            if (k != NCP - 1) tq = mmul(mmul(tq, tq, p, M.q), s, p, M.q);
+            X.wr0[k] = mmul(mmul(bn, tq, p, M.q), M.r2, p, M.q);
+            X.S[k] = mmul(tq, s, p, M.q);
+        }
+    }
+    H.p = p; H.q = M.q; H.one = M.one; H.s = s; H.e = e;
+    if (!(p >> 63)) {                                     // Shoup multiplier of the baby steps below 2^63
+        H.sp = from_mont(s, M);
+        H.ssw = shoup_of_mont(s, M.q);
     }
     H.smul = small_power(b, e);
-    // giant steps per target: ceil(ceil(L/e)/Q) cover every u of every offset
-    const u64 Le = ((u64)job->L + e - 1) / e;
-    H.Mg = (u32)((Le + gm.q - 1) / gm.q);
     hdr[t] = H;
     aux[t] = X;
 }
 
 
-// Kernel 1.  Single job: primes[first, first+count) into records [0, count)
-// with the launch's geometry gm.  Batch (BATCH): the primes of every range as
-// one index space (prefix: prefix sums of the ranges' prime counts); prime i
-// of range r is record r*rcap + i, with its job's sequences and geometry.
+// Kernel 1.  Single job: primes[first, first+count) into records [0, count).
+// Batch (BATCH): the primes of every range as one index space (prefix: prefix
+// sums of the ranges' prime counts); prime i of range r is record r*rcap + i,
+// with its job's sequences.
 template <bool BATCH>
 __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ jobs, const u64 *__restrict__ primes,
                                                      u32 first, u32 count, PrimeHdr *__restrict__ hdr,
-                                                     PrimeAux *__restrict__ aux, u64 *__restrict__ tabs, JobGeom gm,
+                                                     PrimeAux *__restrict__ aux, JobGeom gm,
                                                      const JobGeom *__restrict__ geoms,
                                                      const BatchRange *__restrict__ ranges,
                                                      const u32 *__restrict__ prefix, u32 nr, u32 rcap)
@@ -171,16 +181,57 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
             const u32 r = prefix_find(prefix, nr, i);
             const u32 rec = r * rcap + (i - prefix[r]);
             const u32 jb = ranges[r].job;
-            setup_prime_one(jobs + jb, primes[rec], rec, jb, hdr, aux, tabs, geoms[jb]);
+            setup_prime_one(jobs + jb, primes[rec], rec, jb, hdr, aux, geoms[jb]);
         }
     } else {
         for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += stride)
-            setup_prime_one(jobs, primes[first + t], t, 0, hdr, aux, tabs, gm);
+            setup_prime_one(jobs, primes[first + t], t, 0, hdr, aux, gm);
     }
 }
 
-// Sequence classes, targets and giant-step tables of record w (one warp).
-// tw: this warp's two tables of SPLIT_MAX entries in shared memory.
+// Baby steps per thread for a prime with nk targets of Le giant-step units
+// each: the index k of the per-thread count C >> k in {C, C/2, C/4} (Q' =
+// tpb*(C >> k) baby steps) that minimises Q' + GIANT_COST * (nk * ceil(Le/Q')
+// giant steps + 2 start products per giant thread).  A prime with a large
+// split modulus has few giant steps per target and takes fewer baby steps.
+// tpb and C are powers of two, so every division is a shift.
+constexpr float GIANT_COST = 1.2f;
+__device__ __forceinline__ u32 choose_cp(const JobGeom &gm, u32 nk, u64 Le)
+{
+    u32 best_k = 0;
+    float best = 3.0e38f;
+    const int lq = 31 - __clz(gm.tpb * gm.c);
+    const u32 g0 = gm.tpb / nk;
+    for (u32 k = 0; k < NCP; ++k) {
+        const u64 qp = 1ull << (lq - k);
+        const u64 mg = (Le + qp - 1) >> (lq - k);
+        u64 g = g0 < 1 ? 1 : g0;
+        if (g > mg) g = mg;
+        const float cost = (float)qp + GIANT_COST * ((float)nk * (float)mg + 2.0f * (float)(nk * g));
+        if (cost < best) { best = cost; best_k = k; }
+    }
+    return best_k;
+}
+
+// a[r] = x[r]^ex for r < R, the R chains interleaved (the exponent is the same
+// for every lane and chain, so the loop is uniform over the warp); ex >= 1.
+template <int R>
+__device__ __forceinline__ void mpow_multi(u64 (&a)[4], const u64 (&x)[4], u64 ex, const Mont &M)
+{
+#pragma unroll
+    for (int r = 0; r < R; ++r) a[r] = x[r];
+    for (int bit = 62 - __clzll(ex); bit >= 0; --bit) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r] = mmul(a[r], a[r], M.p, M.q);
+        if ((ex >> bit) & 1) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) a[r] = mmul(a[r], x[r], M.p, M.q);
+        }
+    }
+}
+
+// Sequence classes, targets, baby-step count and the start tables of record w
+// (one warp).  tw: this warp's two tables of SPLIT_MAX entries in shared memory.
 __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 w, u32 lane, PrimeHdr *__restrict__ hdr,
                                             const PrimeAux *__restrict__ aux, u64 *__restrict__ tabs,
                                             u64 *__restrict__ tgt, unsigned short *__restrict__ meta,
@@ -192,41 +243,67 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
         if (lane == 0) atomicAdd(&stats[ST_SKIPPED], 1ull);
         return;
     }
-    const PrimeAux X = aux[w];
+    const PrimeAux &X = aux[w];
     Mont M;
     M.p = H.p; M.q = H.q; M.one = H.one; M.r2 = X.r2;
     const u64 p = H.p;
     const u32 K = job->kcount;
     const u32 e = X.e;
     const u64 mone = p - M.one;
-    // hinv[r] = h^(-r) = h^((e - r) mod e) and wt[r] = b^(nmin + e(Q-1) + r) * R^2, for r < e
+    u64 *tg = tgt + (size_t)w * KSTRIDE;
+    unsigned short *mg_ = meta + (size_t)w * KSTRIDE;
+    // hinv[r] = h^(-r) = h^((e - r) mod e) and, for now, wt[r] = b^r, for r < e
     u64 *hinv = tw, *wt = tw + SPLIT_MAX;
     __syncwarp();                                          // the previous prime's readers are done
     for (u32 r = lane; r < e; r += 32) {
-        hinv[r] = mpow(X.h, (u64)((e - r) % e), M);
-        wt[r] = mmul(X.wr0, mpow(X.bm, (u64)r, M), p, M.q);
+        hinv[r] = mpow_call(X.h, (u64)((e - r) % e), M);
+        wt[r] = mpow_call(X.bm, (u64)r, M);
+    }
+    // z = chi(k) = k^xD for the lane's sequences i = lane + 32r, r < R: one
+    // exponent for the whole warp, R independent chains per lane
+    const u32 R = (K + 31) / 32;
+    u64 z[4];
+    {
+        u64 x[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const u32 i = lane + 32 * r;
+            const u64 kv = (i < K) ? job->k[i] : 1;
+            x[r] = to_mont((kv < p) ? kv : kv % p, M);
+        }
+        if (R == 1) mpow_multi<1>(z, x, X.xD, M);
+        else if (R == 2) mpow_multi<2>(z, x, X.xD, M);
+        else if (R == 3) mpow_multi<3>(z, x, X.xD, M);
+        else mpow_multi<4>(z, x, X.xD, M);
     }
     __syncwarp();
+    // pass 1: the class of every sequence; the kept ones' k mod p and class
+    // offset go to the record (compacted), the target itself once Q' is known
     const u32 nmod = job->nmin % e;
     u32 nk = 0;
     bool divk = false, lost = false;
-    for (u32 i0 = 0; i0 < K; i0 += 32) {
-        const u32 i = i0 + lane;
+#pragma unroll
+    for (int rd = 0; rd < 4; ++rd) {
+        if ((u32)rd >= R) break;
+        const u32 i = lane + 32 * rd;
         bool keep = false;
-        u64 T = 0;
+        u64 kr = 0;
         unsigned short mt = 0;
         if (i < K) {
             const u64 kv = job->k[i];
-            const u64 kr = (kv < p) ? kv : kv % p;
+            kr = (kv < p) ? kv : kv % p;
             if (kr == 0) {
                 divk = true;
             } else {
                 const int ci = job->c[i];
-                // z = chi(k); the target is possible iff (chi(-c)/z)^eo == 1, i.e.
-                // z1^e == chi(-c)^eo with z1 = z^xe; chi(-c) is 1 for c = -1
-                const u64 z1 = mpow(mpow(to_mont(kr, M), X.xD, M), X.xe, M);
+                // the target is possible iff (chi(-c)/z)^eo == 1, i.e.
+                // z1^e == chi(-c)^eo with z1 = z^xe; chi(-c) is 1 for c = -1.
+                // When xe = 1 (eo = e, the usual case) that is exactly "the class
+                // search below finds r", so the power is skipped.
+                const u64 z1 = (X.xe == 1) ? z[rd] : mpow_call(z[rd], X.xe, M);
                 const u64 want = (ci == 1 && (X.flags & AUX_NEG_EO)) ? mone : M.one;
-                if (mpow(z1, (u64)e, M) == want) {
+                const bool pass = (X.xe == 1) || mpow_call(z1, (u64)e, M) == want;
+                if (pass) {
                     // n == r (mod e) where z1 * h^r == chi(-c)^xe
                     const bool neg = (ci == 1) && (X.flags & AUX_NEG_XE);
                     u32 r = e;
@@ -236,11 +313,9 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
                     }
                     if (r < e) {
                         const u32 off = (r + e - nmod) % e;
-                        T = mmul(kr, wt[off], p, M.q);
-                        if (ci == 1) T = mneg(T, p);
                         mt = (unsigned short)(i | (off << 7));
                         keep = true;
-                    } else {
+                    } else if (X.xe != 1) {
                         lost = true;                      // cannot happen: the class exists when the test passes
                     }
                 }
@@ -249,8 +324,8 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
         const u32 km_ = __ballot_sync(0xFFFFFFFFu, keep);
         if (keep) {
             const u32 pos = nk + __popc(km_ & ((1u << lane) - 1));
-            tgt[(size_t)w * KSTRIDE + pos] = T;
-            meta[(size_t)w * KSTRIDE + pos] = mt;
+            tg[pos] = kr;
+            mg_[pos] = mt;
         }
         nk += __popc(km_);
     }
@@ -263,38 +338,117 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
         }
         return;
     }
-    // giant-phase split: G chunks of Lc giant steps per target, numk*G <= tpb
-    const u32 Mg = H.Mg;
+    // baby steps for this prime (the giant-step tables follow in kernel 3)
+    const u64 Le = ((u64)job->L + e - 1) / e;
+    const u32 kc = choose_cp(gm, nk, Le);
+    // targets T = -c * k * b^(nmin + off + e(Q'-1)): wt[r] = b^(nmin + e(Q'-1) + r) * R^2
+    const u64 wr0 = X.wr0[kc];
+    for (u32 r = lane; r < e; r += 32) wt[r] = mmul(wr0, wt[r], p, M.q);
+    __syncwarp();                                          // also orders pass 1's record writes
+    for (u32 j = lane; j < nk; j += 32) {
+        const u32 m = mg_[j];
+        u64 T = mmul(tg[j], wt[m >> 7], p, M.q);
+        if (job->c[m & 0x7Fu] == 1) T = mneg(T, p);
+        tg[j] = T;
+    }
+    if (lane == 0) {
+        hdr[w].numk = nk;
+        hdr[w].cp = gm.c >> kc;
+    }
+}
+
+// Baby- and giant-step tables of record t (one thread): giant steps per target
+// Mg = ceil(ceil(L/e)/Q'), G chunks of Lc steps per target (numk*G <= tpb),
+// A[l] = s^(cp*l), B[l] = s^(32*cp*l) (baby starts), Z1[l] = S^(Lc*l),
+// Z2[l] = S^(32*Lc*l) (giant starts) with S = s^Q', and the Shoup quotient of S.
+// Adds the prime's targets and its search kind to the thread's tallies.
+__device__ __forceinline__ void setup_tabs_one(const JobDev *__restrict__ job, u32 t, PrimeHdr *__restrict__ hdr,
+                                               const PrimeAux *__restrict__ aux, u64 *__restrict__ tabs,
+                                               const JobGeom &gm, u32 &n_targets, u32 &n_full, u32 &n_split)
+{
+    PrimeHdr H = hdr[t];
+    if (H.p == 0) return;
+    const u64 p = H.p, q = H.q;
+    Mont M;
+    M.p = p; M.q = q; M.one = H.one; M.r2 = 0;
+    const u32 e = H.e, cp = H.cp, nk = H.numk;
+    const u32 kc = 31 - __clz(gm.c / cp);
+    const u32 qp = gm.tpb * cp;
+    const u64 Le = ((u64)job->L + e - 1) / e;
+    const u32 Mg = (u32)((Le + qp - 1) / qp);
     u32 G = gm.tpb / nk;
     if (G < 1) G = 1;
     if (G > Mg) G = Mg;
     const u32 Lc = (Mg + G - 1) / G;
     G = (Mg + Lc - 1) / Lc;
-    // Z1[l] = S^(Lc*l), Z2[w] = S^(32*Lc*w), lane l computes entry l of both
-    const u64 z = mpow(H.S, (u64)Lc, M);
-    u64 acc = M.one, pw = z, acc2 = M.one;
-#pragma unroll
-    for (int bit = 0; bit < 5; ++bit) {
-        if ((lane >> bit) & 1) acc = mmul(acc, pw, p, M.q);
-        pw = mmul(pw, pw, p, M.q);
+    const u64 S = aux[t].S[kc];
+    const u64 Sh = mpow(S, (u64)(Lc >> 1), M);            // start of a thread's second giant chain
+    const u64 z = (Lc & 1) ? mmul(mmul(Sh, Sh, p, q), S, p, q) : mmul(Sh, Sh, p, q);   // S^Lc
+    u64 u = H.s;                                           // s^cp, cp a power of two
+    for (u32 c = cp; c > 1; c >>= 1) u = mmul(u, u, p, q);
+    u64 *tb = tabs + (size_t)t * TABS;
+    // four power tables, two chains at a time
+    u64 a = M.one, b = M.one;
+    for (int l = 0; l < 32; ++l) {
+        tb[l] = a;
+        tb[64 + l] = b;
+        a = mmul(a, u, p, q);
+        b = mmul(b, z, p, q);
     }
-    // pw = z^32
-#pragma unroll
-    for (int bit = 0; bit < 5; ++bit) {
-        if ((lane >> bit) & 1) acc2 = mmul(acc2, pw, p, M.q);
-        pw = mmul(pw, pw, p, M.q);
+    const u64 u32p = a, z32 = b;                           // u^32, z^32
+    a = M.one;
+    b = M.one;
+    for (int l = 0; l < 32; ++l) {
+        tb[32 + l] = a;
+        tb[96 + l] = b;
+        a = mmul(a, u32p, p, q);
+        b = mmul(b, z32, p, q);
     }
-    u64 *tb = tabs + (size_t)w * TABS;
-    tb[64 + lane] = acc;
-    tb[96 + lane] = acc2;
-    const u64 sh = mpow(H.S, (u64)(Lc >> 1), M);
-    if (lane == 0) {
-        hdr[w].numk = nk;
-        hdr[w].G = G;
-        hdr[w].Lc = Lc;
-        hdr[w].Sh = sh;
-        atomicAdd(&stats[ST_TARGETS], (u64)nk);
-        atomicAdd(&stats[e >= 2 ? ST_PARITY : ST_FULL], 1ull);
+    PrimeHdr &h = hdr[t];
+    h.G = G;
+    h.Lc = Lc;
+    h.Mg = Mg;
+    h.S = S;
+    h.Sh = Sh;
+    if (!(p >> 63)) {                                      // Shoup multiplier of the giant steps below 2^63
+        h.Sp = from_mont(S, M);
+        h.Sw = shoup_of_mont(S, q);
+    }
+    n_targets += nk;
+    if (e >= 2) ++n_split; else ++n_full;
+}
+
+// Kernel 3: one thread per prime (indexing as kernel 1).
+template <bool BATCH>
+__global__ void __launch_bounds__(256) k_setup_tabs(const JobDev *__restrict__ jobs, PrimeHdr *__restrict__ hdr,
+                                                    const PrimeAux *__restrict__ aux, u32 count,
+                                                    u64 *__restrict__ tabs, u64 *__restrict__ stats, JobGeom gm,
+                                                    const JobGeom *__restrict__ geoms,
+                                                    const BatchRange *__restrict__ ranges,
+                                                    const u32 *__restrict__ prefix, u32 nr, u32 rcap)
+{
+    const u32 stride = gridDim.x * blockDim.x;
+    u32 nt = 0, nf = 0, ns = 0;
+    if constexpr (BATCH) {
+        const u32 total = prefix[nr];
+        for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+            const u32 r = prefix_find(prefix, nr, i);
+            const u32 rec = r * rcap + (i - prefix[r]);
+            const u32 jb = ranges[r].job;
+            setup_tabs_one(jobs + jb, rec, hdr, aux, tabs, geoms[jb], nt, nf, ns);
+        }
+    } else {
+        for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += stride)
+            setup_tabs_one(jobs, t, hdr, aux, tabs, gm, nt, nf, ns);
+    }
+    // one atomic per warp and counter
+    nt = __reduce_add_sync(0xFFFFFFFFu, nt);
+    nf = __reduce_add_sync(0xFFFFFFFFu, nf);
+    ns = __reduce_add_sync(0xFFFFFFFFu, ns);
+    if ((threadIdx.x & 31) == 0) {
+        if (nt) atomicAdd(&stats[ST_TARGETS], (u64)nt);
+        if (nf) atomicAdd(&stats[ST_FULL], (u64)nf);
+        if (ns) atomicAdd(&stats[ST_PARITY], (u64)ns);
     }
 }
 
@@ -334,7 +488,7 @@ cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 co
 {
     if (count == 0) return cudaSuccess;
     const JobGeom gm = job_geom(geom);
-    k_setup_prime<false><<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, tabs, gm,
+    k_setup_prime<false><<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, gm,
                                                               nullptr, nullptr, nullptr, 0, 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -342,6 +496,10 @@ cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 co
     k_setup_k<false><<<(count + wpb - 1) / wpb, SETUP_TPB, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, tgt,
                                                                    meta, stats, err, gm, nullptr, nullptr, nullptr, 0,
                                                                    0);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_setup_tabs<false><<<(count + 255) / 256, 256, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, stats, gm,
+                                                             nullptr, nullptr, nullptr, 0, 0);
     return cudaGetLastError();
 }
 
@@ -351,12 +509,16 @@ cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const B
 {
     JobGeom gm{};
     // full-device grids; the kernels stride over the primes of every range
-    k_setup_prime<true><<<sms * 4, 256, 0, st>>>(jobs, primes, 0, 0, hdr, (PrimeAux *)aux, tabs, gm, geoms, ranges,
+    k_setup_prime<true><<<sms * 4, 256, 0, st>>>(jobs, primes, 0, 0, hdr, (PrimeAux *)aux, gm, geoms, ranges,
                                                  prefix_p, nranges, rcap);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_setup_k<true><<<sms * 4, SETUP_TPB, 0, st>>>(jobs, hdr, (const PrimeAux *)aux, 0, tabs, tgt, meta, stats, err,
                                                    gm, geoms, ranges, prefix_p, nranges, rcap);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_setup_tabs<true><<<sms * 4, 256, 0, st>>>(jobs, hdr, (const PrimeAux *)aux, 0, tabs, stats, gm, geoms, ranges,
+                                                prefix_p, nranges, rcap);
     return cudaGetLastError();
 }
 

@@ -41,9 +41,11 @@ class Unit:
 
 def cost_per_prime(q, kcount, L):
     """Model cost of one prime in baby-step units for Q baby steps (the library's
-    geometry model: Q baby steps plus the giant steps of the surviving targets)."""
-    m = -(-L // q)
-    return 1.15 * q + 1.2 * 0.6 * kcount * 0.75 * m
+    geometry model: Q baby steps plus the giant steps of the surviving targets,
+    each over one class of n modulo the prime's split modulus, about 0.15 L/Q
+    steps and at least one)."""
+    m = max(1.0, 0.15 * L / q + 0.5)
+    return 1.15 * q + 1.2 * 0.6 * kcount * m
 
 
 class Server:
