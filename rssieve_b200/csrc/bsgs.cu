@@ -407,8 +407,8 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
     constexpr u32 Q = TPB * C;
     static_assert(Q <= 65536, "baby indices are stored in 16 bits");
     static_assert(NB <= 65536, "bucket indices are packed into 16 bits");
-    constexpr int IBMAX = (C < 8) ? C : 8;                        // values inserted per round
-    static_assert(C % IBMAX == 0 && IBMAX % 4 == 0, "cp in {C, C/2, C/4} must split into rounds");
+    constexpr int IBMAX = 8;                                      // values inserted per round (two chains)
+    static_assert(C >= IBMAX, "cp in {C, C/2, C/4} splits into rounds of IBMAX/2, IBMAX/4 or IBMAX/8 per chain");
     const Table T = Smem<TPB, NB>::table();
     u64 *s_start = Smem<TPB, NB>::start();
     u64 *s_Z = Smem<TPB, NB>::zs();
@@ -497,51 +497,64 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             // Speculative: ord(s) < Q' is only known after the barrier; then the
             // table (which may hold repeats) is rebuilt from j < ord.
             const u64 one = R.hdr.one;
-            u64 x = mmul(R.tabs[tid & 31], R.tabs[32 + (tid >> 5)], p, q);   // s^(cp*tid)
-            s_start[tid] = x;
+            const u64 x0 = mmul(R.tabs[tid & 31], R.tabs[32 + (tid >> 5)], p, q);   // s^(cp*tid)
+            s_start[tid] = x0;
             u32 spill = 0;
-            // The step kind is uniform per prime (b^e = 2, 4 or other) and is
-            // chosen once, so the loop body carries no dispatch; the first j > 0
-            // with y_j = 1 is kept per thread and merged with one atomicMin.
-            // Other multipliers take Shoup's product by the plain s below 2^63
-            // (the same residues as the Montgomery product verify() uses).
+            // Two chains per thread, j in [tid*cp, tid*cp + cp/2) and the next
+            // cp/2 (started from s^(cp/2) further), so the two products of a step
+            // are independent.  The step kind is uniform per prime (b^e = 2, 4 or
+            // other) and is chosen once, so the loop body carries no dispatch;
+            // the least j > 0 with y_j = 1 is kept per thread and merged with one
+            // atomicMin.  Other multipliers take Shoup's product by the plain s
+            // below 2^63 (the same residues as the Montgomery product verify()
+            // uses).
             u32 minj = 0xFFFFFFFFu;
             const u64 ssw = R.hdr.ssw;
             const u64 sp = R.hdr.sp;
-            // cp is C, C/2 or C/4: IB values are hashed and stepped, then
-            // inserted, per round (IB = 8, or cp when it is smaller)
+            const u32 half = cp >> 1;
+            u64 xa = x0, xb = mmul(x0, R.hdr.u2, p, q);
+            // IB2 values of each chain are hashed and stepped, then inserted, per
+            // round (IB2 = IBMAX/2, or cp/2 when it is smaller)
             auto babies = [&](auto kind, auto ibc) {
                 constexpr int K = decltype(kind)::value;          // 2, 4: doublings; 1: Shoup; 0: baby_step
-                constexpr int IB = decltype(ibc)::value;
+                constexpr int IB2 = decltype(ibc)::value;
+                auto step = [&](u64 v) -> u64 {
+                    if (K == 0) return baby_step(v, smul, s, p, q);
+                    if (K == 1) return shoup_mul(v, sp, ssw, p);
+                    if (MODE == 1) { v = dbl63(v, p); return (K == 4) ? dbl63(v, p) : v; }
+                    v = madd(v, v, p);
+                    return (K == 4) ? madd(v, v, p) : v;
+                };
 #pragma unroll 1
-                for (u32 h0 = 0; h0 < cp; h0 += IB) {
-                    u32 bf[IB], old[IB];                          // bucket << 16 | fingerprint; claimed slot
+                for (u32 h0 = 0; h0 < half; h0 += IB2) {
+                    u32 bf[2 * IB2], old[2 * IB2];                // bucket << 16 | fingerprint; claimed slot
 #pragma unroll
-                    for (int i = 0; i < IB; ++i) {
-                        const u32 j = tid * cp + h0 + i;
-                        if (j != 0 && x == one && minj == 0xFFFFFFFFu) minj = j;
+                    for (int i = 0; i < IB2; ++i) {
+                        const u32 ja = tid * cp + h0 + i, jb = ja + half;
+                        if (ja != 0 && xa == one) minj = min(minj, ja);
+                        if (xb == one) minj = min(minj, jb);
                         u32 bk, fp;
-                        tab_hash<NB>(x, bk, fp);
-                        bf[i] = (bk << 16) | fp;
-                        if (K == 0) x = baby_step(x, smul, s, p, q);
-                        else if (K == 1) x = shoup_mul(x, sp, ssw, p);
-                        else if (MODE == 1) { x = dbl63(x, p); if (K == 4) x = dbl63(x, p); }
-                        else { x = madd(x, x, p); if (K == 4) x = madd(x, x, p); }
+                        tab_hash<NB>(xa, bk, fp);
+                        bf[2 * i] = (bk << 16) | fp;
+                        tab_hash<NB>(xb, bk, fp);
+                        bf[2 * i + 1] = (bk << 16) | fp;
+                        xa = step(xa);
+                        xb = step(xb);
                     }
 #pragma unroll
-                    for (int i = 0; i < IB; ++i) old[i] = tab_claim(T, bf[i] >> 16);
+                    for (int i = 0; i < 2 * IB2; ++i) old[i] = tab_claim(T, bf[i] >> 16);
 #pragma unroll
-                    for (int i = 0; i < IB; ++i) {
-                        const u32 j = tid * cp + h0 + i;
+                    for (int i = 0; i < 2 * IB2; ++i) {
+                        const u32 j = tid * cp + h0 + (i >> 1) + ((i & 1) ? half : 0u);
                         const u32 bk = bf[i] >> 16, fp = bf[i] & 0xFFFFu;
                         if (!tab_fill(T, bk, old[i], fp, j)) spill |= insert_walk<NB>(bk, fp, j, BSGS_SPEC_PROBE);
                     }
                 }
             };
             auto babies_cp = [&](auto kind) {
-                if (cp >= IBMAX) babies(kind, std::integral_constant<int, IBMAX>{});
-                else if (cp >= IBMAX / 2) babies(kind, std::integral_constant<int, IBMAX / 2>{});
-                else babies(kind, std::integral_constant<int, IBMAX / 4>{});
+                if (half >= IBMAX / 2) babies(kind, std::integral_constant<int, IBMAX / 2>{});
+                else if (half >= IBMAX / 4) babies(kind, std::integral_constant<int, IBMAX / 4>{});
+                else babies(kind, std::integral_constant<int, IBMAX / 8>{});
             };
             if (smul == 2) babies_cp(std::integral_constant<int, 2>{});
             else if (smul == 4) babies_cp(std::integral_constant<int, 4>{});

@@ -40,6 +40,19 @@ RS_DEV u64 shoup_mul(u64 x, u64 w, u64 wp, u64 p)
     return (r >= p) ? r - p : r;
 }
 
+// Montgomery product without the final correction, for p < 2^62: for a, b in
+// [0, 2p), (a*b - m*p)/2^64 lies in (-p, p), so adding p gives a result in
+// (0, 2p) congruent to a*b*2^-64.  Chains of products stay in [0, 2p); one
+// conditional subtraction (mred) makes the end result canonical.
+RS_DEV u64 mmul_lazy(u64 a, u64 b, u64 p, u64 q)
+{
+    const u64 lo = a * b;
+    const u64 hi = __umul64hi(a, b);
+    const u64 m = lo * q;
+    return hi + p - __umul64hi(m, p);
+}
+RS_DEV u64 mred(u64 x, u64 p) { return (x >= p) ? x - p : x; }
+
 // Shoup's quotient floor(w * 2^64 / p) of the plain value w < p < 2^63, from
 // its Montgomery form wm = w * 2^64 mod p: w * 2^64 = wp * p + wm, so
 // wp * p == -wm (mod 2^64) and wp = -wm * p^-1 mod 2^64 (q = p^-1 mod 2^64).

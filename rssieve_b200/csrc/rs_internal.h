@@ -110,7 +110,7 @@ struct JobDev {
     u32 *bitmap;         // kcount * words
 };
 
-struct PrimeHdr {        // 112 bytes (a 16-byte multiple: copied by TMA bulk copies)
+struct PrimeHdr {        // 128 bytes (a 16-byte multiple: copied by TMA bulk copies)
     u64 p;               // 0 = skipped
     u64 q;               // p^-1 mod 2^64
     u64 one;             // 2^64 mod p
@@ -127,8 +127,10 @@ struct PrimeHdr {        // 112 bytes (a 16-byte multiple: copied by TMA bulk co
     u64 Sw;              // floor(Sp*2^64/p), Sp = s^Q' mod p (plain), for Shoup giant steps; 0 when p >= 2^63
     u64 ssw;             // floor(sp*2^64/p), sp = s mod p (plain), for Shoup baby steps; 0 when p >= 2^63
     u64 sp, Sp;          // s and s^Q' as plain residues, the Shoup multipliers (0 when p >= 2^63)
+    u64 u2;              // Montgomery s^(cp/2): start offset of a thread's second baby chain
+    u64 pad2_;
 };
-static_assert(sizeof(PrimeHdr) == 112, "PrimeHdr is copied in 16-byte units");
+static_assert(sizeof(PrimeHdr) == 128, "PrimeHdr is copied in 16-byte units");
 
 struct FactorRec {       // one claimed term: p | k[seq]*b^n + c[seq]
     u64 p;

@@ -108,7 +108,7 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
 {
     PrimeHdr H;
     H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.job = jb;
-    H.Mg = 0; H.cp = 0; H.Sh = 0; H.Sw = 0; H.ssw = 0; H.sp = 0; H.Sp = 0;
+    H.Mg = 0; H.cp = 0; H.Sh = 0; H.Sw = 0; H.ssw = 0; H.sp = 0; H.Sp = 0; H.u2 = 0; H.pad2_ = 0;
     const Mont M = mont_init(p);
     const u32 b = job->base;
     const u64 bm = to_mont(b, M);
@@ -215,19 +215,34 @@ __device__ __forceinline__ u32 choose_cp(const JobGeom &gm, u32 nk, u64 Le)
 
 // a[r] = x[r]^ex for r < R, the R chains interleaved (the exponent is the same
 // for every lane and chain, so the loop is uniform over the warp); ex >= 1.
-template <int R>
+// LAZY (p < 2^62): the chains stay in [0, 2p) without per-product corrections.
+template <int R, bool LAZY>
 __device__ __forceinline__ void mpow_multi(u64 (&a)[4], const u64 (&x)[4], u64 ex, const Mont &M)
 {
+    auto mul = [&](u64 u, u64 v) { return LAZY ? mmul_lazy(u, v, M.p, M.q) : mmul(u, v, M.p, M.q); };
 #pragma unroll
     for (int r = 0; r < R; ++r) a[r] = x[r];
     for (int bit = 62 - __clzll(ex); bit >= 0; --bit) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[r] = mmul(a[r], a[r], M.p, M.q);
+        for (int r = 0; r < R; ++r) a[r] = mul(a[r], a[r]);
         if ((ex >> bit) & 1) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) a[r] = mmul(a[r], x[r], M.p, M.q);
+            for (int r = 0; r < R; ++r) a[r] = mul(a[r], x[r]);
         }
     }
+    if (LAZY) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r] = mred(a[r], M.p);
+    }
+}
+
+template <bool LAZY>
+__device__ __forceinline__ void mpow_lanes(u32 R, u64 (&a)[4], const u64 (&x)[4], u64 ex, const Mont &M)
+{
+    if (R == 1) mpow_multi<1, LAZY>(a, x, ex, M);
+    else if (R == 2) mpow_multi<2, LAZY>(a, x, ex, M);
+    else if (R == 3) mpow_multi<3, LAZY>(a, x, ex, M);
+    else mpow_multi<4, LAZY>(a, x, ex, M);
 }
 
 // Sequence classes, targets, baby-step count and the start tables of record w
@@ -271,10 +286,8 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
             const u64 kv = (i < K) ? job->k[i] : 1;
             x[r] = to_mont((kv < p) ? kv : kv % p, M);
         }
-        if (R == 1) mpow_multi<1>(z, x, X.xD, M);
-        else if (R == 2) mpow_multi<2>(z, x, X.xD, M);
-        else if (R == 3) mpow_multi<3>(z, x, X.xD, M);
-        else mpow_multi<4>(z, x, X.xD, M);
+        if (p >> 62) mpow_lanes<false>(R, z, x, X.xD, M);
+        else mpow_lanes<true>(R, z, x, X.xD, M);
     }
     __syncwarp();
     // pass 1: the class of every sequence; the kept ones' k mod p and class
@@ -384,8 +397,9 @@ __device__ __forceinline__ void setup_tabs_one(const JobDev *__restrict__ job, u
     const u64 S = aux[t].S[kc];
     const u64 Sh = mpow(S, (u64)(Lc >> 1), M);            // start of a thread's second giant chain
     const u64 z = (Lc & 1) ? mmul(mmul(Sh, Sh, p, q), S, p, q) : mmul(Sh, Sh, p, q);   // S^Lc
-    u64 u = H.s;                                           // s^cp, cp a power of two
-    for (u32 c = cp; c > 1; c >>= 1) u = mmul(u, u, p, q);
+    u64 u2 = H.s;                                          // s^(cp/2) and s^cp, cp a power of two >= 2
+    for (u32 c = cp >> 1; c > 1; c >>= 1) u2 = mmul(u2, u2, p, q);
+    const u64 u = mmul(u2, u2, p, q);
     u64 *tb = tabs + (size_t)t * TABS;
     // four power tables, two chains at a time
     u64 a = M.one, b = M.one;
@@ -410,6 +424,7 @@ __device__ __forceinline__ void setup_tabs_one(const JobDev *__restrict__ job, u
     h.Mg = Mg;
     h.S = S;
     h.Sh = Sh;
+    h.u2 = u2;
     if (!(p >> 63)) {                                      // Shoup multiplier of the giant steps below 2^63
         h.Sp = from_mont(S, M);
         h.Sw = shoup_of_mont(S, q);
