@@ -62,6 +62,25 @@ def mulmod_rates(counters, seconds, peak_g):
             "giant_frac_of_mulmod_peak": g / (peak_g * 1e9)}
 
 
+def job_of(name, seed, W):
+    """(job, first p, workload label) of the timed steps' job."""
+    if name == "config2":
+        return W.config2(seed), P_START, WORKLOAD
+    if name == "config1":
+        j = W.config1(1)
+        return j, j["prange"][0], "config1 job: 8 seqs k*2^n-1, k odd < 2^20, n in [1e5,3e5), p windows from 1e12"
+    if name == "config4":
+        j = W.config4()
+        return j, j["prange"][0], ("config4 job: 20 seqs b=5, k even < 2^40, n in [1e6,3e6), p windows from "
+                                   "2^64-2^36")
+    if name.startswith("config3:"):
+        i = int(name.split(":")[1])
+        j = W.config3(3)[i]
+        return j, j["prange"][0], "config3 job %d: %d seqs b=%d, n in [%d,%d], p windows from %d" % (
+            i, len(j["k"]), j["base"], j["nmin"], j["nmax"], j["prange"][0])
+    raise ValueError("unknown --job %s" % name)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -75,6 +94,12 @@ def parse():
     ap.add_argument("--no-forms", action="store_true",
                     help="skip the batched (configs 2, 3, 4) and served (config 5) forms")
     ap.add_argument("--serve-rates", default="", help="extra arrival rates (units/s, comma-separated) to serve")
+    ap.add_argument("--form", default="",
+                    help="run only this form (config1, batched, batched_config2, batched_config4, served, "
+                         "served_stated) and print its result, for profiling it on its own")
+    ap.add_argument("--job", default="config2",
+                    help="job of the timed steps: config2 (the benchmark), config1, config4 or config3:<index>; "
+                         "the others are for profiling single kernels on those shapes")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU-baseline sample length")
     return ap.parse_args()
 
@@ -221,7 +246,8 @@ def measure_one_job_batched(torch, rs, W, peak_g, job, p0, width_log2, nsplit, l
     """One job over one p-window through the single-job path and through the batch
     (a resident copy of the job cloned over nsplit range slots, at the Q the
     single-job tuner measured for the job's shape); CUDA events on one side stream
-    bracket each, the batch's upload and clone included."""
+    bracket the sieving of each, with the job already resident on the device
+    (the single-job load and the batch's upload and clone outside)."""
     import numpy as np
     seqs = W.seqs_of(job)
     p1 = p0 + (1 << width_log2)
@@ -244,10 +270,10 @@ def measure_one_job_batched(torch, rs, W, peak_g, job, p0, width_log2, nsplit, l
     sv.close()
     b = rs.Batch(torch.cuda.current_device(), max_jobs=2, range_slots=nsplit)
     b.set_stream(st.cuda_stream)
-    torch.cuda.synchronize()
-    ev[2].record(st)
     t = b.add(seqs, p0, p0)
     j = b.add_clone(t, p0, p1, nsplit)
+    torch.cuda.synchronize()
+    ev[2].record(st)                           # the job resident on both sides: sieving only
     b.run(0)
     ev[3].record(st)
     torch.cuda.synchronize()
@@ -363,6 +389,36 @@ def measure_served(rs, W, serve, peak_g, seed=5, nunits=60, rate=8.0, width_log2
     return st
 
 
+def forms_of(torch, rs, W, peak, value, job, names):
+    """The batched and served forms (and config 1) named in names."""
+    from rssieve_b200 import serve
+    makers = {
+        "config1": lambda: measure_config1(torch, rs, W, peak),
+        "batched": lambda: measure_batched(torch, rs, W, peak),
+        "batched_config2": lambda: measure_one_job_batched(torch, rs, W, peak, job, P_START + (1 << 37), 29, 32,
+                                                           "config2 job"),
+        "batched_config4": lambda: measure_one_job_batched(
+            torch, rs, W, peak, W.config4(), (1 << 64) - (1 << 36), 30, 32,
+            "config4 job (b=5, 20 seqs, k even < 2^40, p near 2^64)"),
+        "served": lambda: measure_served(rs, W, serve, peak),
+        "served_stated": lambda: measure_served(
+            rs, W, serve, peak, seed=6, nunits=5, width_log2=(30, 31), rho=0.5, primes_per_s=value,
+            label="config5 units at the lower end of their stated widths: 5 units of 2^U{30..31} over 16 files, "
+                  "starts log-uniform in [2^44, 2^62], Poisson arrivals at the rate that loads the GPU to 0.5"),
+    }
+    return {n: makers[n]() for n in names}
+
+
+def run_form(args, torch):
+    """One form on its own (no timed steps), for profiling."""
+    import rssieve_b200 as rs
+    from rssieve_b200 import workloads as W
+    with rs.Sieve(torch.cuda.current_device()) as sv:
+        peak = sv.mulmod_peak()
+    out = forms_of(torch, rs, W, peak, 1.5e7, W.config2(args.seed), [args.form])
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -392,6 +448,8 @@ def main():
     rank, world, local = dist_env()
     import torch
     torch.cuda.set_device(local)
+    if args.form:
+        return run_form(args, torch)
     if world > 1:
         import datetime
         import torch.distributed as dist
@@ -418,7 +476,7 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
         return float(t.item())
 
-    job = W.config2(args.seed)
+    job, p_start, workload = job_of(args.job, args.seed, W)
     seqs = W.seqs_of(job)
     stream = torch.cuda.current_stream()
     sv = rs.Sieve(local)
@@ -431,7 +489,7 @@ def main():
     width = 1 << args.width
     # disjoint windows per rank: rank r takes windows r, r+world, ...
     nwin = args.warmup + args.steps
-    windows = [(P_START + (i * world + rank) * width, P_START + (i * world + rank + 1) * width) for i in range(nwin)]
+    windows = [(p_start + (i * world + rank) * width, p_start + (i * world + rank + 1) * width) for i in range(nwin)]
     l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     for i in range(args.warmup):
@@ -482,7 +540,7 @@ def main():
         bm = seqs.bitmap
         cudart = torch.cuda.cudart()
         cudart.cudaHostRegister(bm.ctypes.data, bm.nbytes, 0)
-        ewin = [(P_START + ((nwin + i) * world + rank) * width, P_START + ((nwin + i) * world + rank + 1) * width)
+        ewin = [(p_start + ((nwin + i) * world + rank) * width, p_start + ((nwin + i) * world + rank + 1) * width)
                 for i in range(args.steps)]
         sv.load(seqs)
         sv.run(*ewin[0])                               # warm the load/run/fetch path once
@@ -513,21 +571,11 @@ def main():
 
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
-        from rssieve_b200 import serve
-        forms = {"config1": measure_config1(torch, rs, W, peak),
-                 "batched": measure_batched(torch, rs, W, peak),
-                 "batched_config2": measure_one_job_batched(torch, rs, W, peak, job, P_START + (1 << 37), 29, 32,
-                                                            "config2 job"),
-                 "batched_config4": measure_one_job_batched(torch, rs, W, peak, W.config4(), (1 << 64) - (1 << 36),
-                                                            30, 32,
-                                                            "config4 job (b=5, 20 seqs, k even < 2^40, p near 2^64)"),
-                 "served": measure_served(rs, W, serve, peak)}
-        forms["served_stated"] = measure_served(
-            rs, W, serve, peak, seed=6, nunits=5, width_log2=(30, 31), rho=0.5, primes_per_s=value,
-            label="config5 units at the lower end of their stated widths: 5 units of 2^U{30..31} over 16 files, "
-                  "starts log-uniform in [2^44, 2^62], Poisson arrivals at the rate that loads the GPU to 0.5")
+        forms = forms_of(torch, rs, W, peak, value, W.config2(args.seed),
+                         ["config1", "batched", "batched_config2", "batched_config4", "served", "served_stated"])
         rates = [float(x) for x in args.serve_rates.split(",") if x] if args.serve_rates else []
         if rates:
+            from rssieve_b200 import serve
             forms["served_sweep"] = [measure_served(rs, W, serve, peak, rate=r) for r in rates]
 
     # work per prime against the reference's parameter rule on the same primes: its Q
@@ -544,7 +592,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "primes/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "p_window_log2": args.width, "seed": args.seed,
+            "config": {"workload": workload, "p_window_log2": args.width, "seed": args.seed,
                        "baby_steps": baby_q, "baby_steps_tuned": not tuning,
                        "l2": "flushed between steps (256 MiB write outside the step events)",
                        "parallelism": "p-range windows per rank" if world > 1 else "1 GPU"},

@@ -185,6 +185,7 @@ struct PrimeCtx {
 };
 extern __shared__ __align__(128) unsigned char smem_raw[];
 __shared__ BsgsArgs s_args;
+__shared__ BsgsArgs s_args_next;                         // batch launches: the job arguments of the next prime
 __shared__ PrimeCtx s_ctx;
 __shared__ unsigned long long s_cands, s_dups, s_facs;   // per-CTA totals
 __shared__ unsigned long long s_baby, s_giant, s_small;  // per-CTA totals kept by thread 0
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
     u64 *s_Z = Smem<TPB, NB>::zs();
     RecBuf *rec = Smem<TPB, NB>::rec();                           // two staging buffers
     __shared__ __align__(8) u64 s_bar[3];                        // [2]: never completed (failure test)
-    __shared__ u32 s_idx[2], s_order, s_spill, s_abort;
+    __shared__ u32 s_idx[2], s_order, s_spill, s_abort, s_claim;
     const u32 wait_bound = a.wait_bound ? a.wait_bound : WAIT_BOUND;
     u32 pend_buf = 0, pend_par = 0;                               // the copy waited for when aborting
 
@@ -443,6 +444,8 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         const u32 i0 = slot_of(atomicAdd(work_ctr, 1u));
         s_idx[0] = i0;
         if (i0 != NONE) fetch(0, i0);
+        s_claim = slot_of(atomicAdd(work_ctr, 1u));              // the prime after it, resolved ahead
+        if (BATCH && i0 != NONE) s_args_next = job_args[hdr[i0].job];
     }
     __syncthreads();
 
@@ -469,22 +472,22 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
         const u64 p = R.hdr.p, q = R.hdr.q, s = R.hdr.s;
         const u32 e = R.hdr.e, smul = R.hdr.smul;
         const u32 cp = R.hdr.cp;                                  // baby steps per thread for this prime
-        // claim the next prime; the result is consumed after the table clear,
-        // so this warp keeps issuing while the atomic is in flight
-        u32 nxt = 0;
+        // The next prime's index (and, for a batch, its job's arguments) were
+        // claimed and resolved during the previous prime, off the barriers'
+        // critical path: thread 0 only copies them here.
         if (tid == 0) {
             s_order = 0xFFFFFFFFu;
             s_nsol = 0;
             s_spill = 0;
             s_ctx.p = p; s_ctx.q = q; s_ctx.s = s; s_ctx.smul = smul; s_ctx.e = e;
             s_ctx.cp = cp; s_ctx.qp = TPB * cp;
-            if (BATCH) s_args = job_args[R.hdr.job];
-            nxt = slot_of(atomicAdd(work_ctr, 1u));
+            if (BATCH) s_args = s_args_next;
         }
         if (live) clear_table(T, NB);
         __syncthreads();
         if (s_abort) break;
         if (tid == 0) {
+            const u32 nxt = s_claim;
             s_idx[buf ^ 1] = nxt;
             if (nxt != NONE) {                                    // rec[buf^1] was last read before the previous barrier
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -564,6 +567,14 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             if (spill) s_spill = 1;
         }
         __syncthreads();
+        // the last thread (idle in the giant phase unless every thread has a
+        // chunk) claims the prime after next and loads the next prime's job
+        // arguments; both are read after this prime's last barrier
+        if (tid == TPB - 1) {
+            s_claim = slot_of(atomicAdd(work_ctr, 1u));
+            const u32 nx = s_idx[buf ^ 1];
+            if (BATCH && nx != NONE) s_args_next = job_args[hdr[nx].job];
+        }
         const u32 order = s_order;
         const u32 Mg = R.hdr.Mg;
         if (live) {

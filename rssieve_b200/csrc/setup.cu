@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
 // giant steps + 2 start products per giant thread).  A prime with a large
 // split modulus has few giant steps per target and takes fewer baby steps.
 // tpb and C are powers of two, so every division is a shift.
-constexpr float GIANT_COST = 1.2f;
+constexpr float GIANT_COST = 0.8f;
 __device__ __forceinline__ u32 choose_cp(const JobGeom &gm, u32 nk, u64 Le)
 {
     u32 best_k = 0;
