@@ -53,6 +53,20 @@ RS_DEV u64 mmul_lazy(u64 a, u64 b, u64 p, u64 q)
 }
 RS_DEV u64 mred(u64 x, u64 p) { return (x >= p) ? x - p : x; }
 
+// mmul_lazy(a, a) with the square formed from three 32x32 products instead of
+// a general 64x64 product: a = a1*2^32 + a0 < 2^63 gives a^2 = a1^2*2^64 +
+// (2*a0*a1)*2^32 + a0^2, where 2*a0*a1 < 2^64 since a1 < 2^31.
+RS_DEV u64 msqr_lazy(u64 a, u64 p, u64 q)
+{
+    const u32 a0 = (u32)a, a1 = (u32)(a >> 32);
+    const u64 l = (u64)a0 * a0;
+    const u64 m = (u64)a0 * a1;
+    const u64 lo = l + (m << 33);
+    const u64 hi = (u64)a1 * a1 + (m >> 31) + (lo < l ? 1u : 0u);
+    const u64 t = lo * q;
+    return hi + p - __umul64hi(t, p);
+}
+
 // Shoup's quotient floor(w * 2^64 / p) of the plain value w < p < 2^63, from
 // its Montgomery form wm = w * 2^64 mod p: w * 2^64 = wp * p + wm, so
 // wp * p == -wm (mod 2^64) and wp = -wm * p^-1 mod 2^64 (q = p^-1 mod 2^64).

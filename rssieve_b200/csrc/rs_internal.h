@@ -30,7 +30,7 @@ constexpr int NGEOM = 5;
 constexpr BsgsGeom BSGS_GEOMS[NGEOM] = {
     {16384, 1024, 16, 6144},   // 1 CTA per SM
     {8192, 512, 16, 2944},     // 2
-    {4096, 256, 16, 1408},     // 4
+    {4096, 256, 16, 1376},     // 4 (with the 2.2 KB record buffers, 1408 buckets would leave room for 3)
     {2048, 256, 8, 704},       // 4
     {1024, 128, 8, 352},       // 8
 };

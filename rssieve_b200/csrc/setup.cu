@@ -224,7 +224,7 @@ __device__ __forceinline__ void mpow_multi(u64 (&a)[4], const u64 (&x)[4], u64 e
     for (int r = 0; r < R; ++r) a[r] = x[r];
     for (int bit = 62 - __clzll(ex); bit >= 0; --bit) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[r] = mul(a[r], a[r]);
+        for (int r = 0; r < R; ++r) a[r] = LAZY ? msqr_lazy(a[r], M.p, M.q) : mmul(a[r], a[r], M.p, M.q);
         if ((ex >> bit) & 1) {
 #pragma unroll
             for (int r = 0; r < R; ++r) a[r] = mul(a[r], x[r]);
