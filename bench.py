@@ -579,12 +579,14 @@ def main():
             forms["served_sweep"] = [measure_served(rs, W, serve, peak, rate=r) for r in rates]
 
     # work per prime against the reference's parameter rule on the same primes: its Q
-    # baby steps per searched prime, and the giant steps scaled by its M over ours
+    # baby steps per searched prime, and per surviving target its M giant steps when b
+    # is a quadratic residue mod p and MM when not (the parity split; each for about
+    # half the primes), with the targets that survive here (the reference's filters,
+    # which the character test here contains, keep at least as many)
     rp = reference_params(job["nmin"], job["nmax"])
     searched = tot["full"] + tot["parity"]
-    m_ours = -(-(job["nmax"] - job["nmin"] + 1) // baby_q)
     work_ours = tot["baby"] + tot["giant"]
-    work_ref = rp["Q"] * searched + tot["giant"] * rp["M"] / m_ours
+    work_ref = rp["Q"] * searched + tot["targets"] * 0.5 * (rp["M"] + rp["MM"])
     rp["work_per_prime_est"] = work_ref / max(tot["primes"], 1)
 
     if rank == 0:
