@@ -9,7 +9,8 @@
 //
 //   k_batch_windows  next window of every range (sized for ~0.6*RCAP primes)
 //   k_sieve_batch    segmented sieve, blockIdx.y = range
-//   k_mr_batch       Miller-Rabin over the survivors of every range at once
+//   k_mr_batch_sprp, k_mr_batch_lucas  Baillie-PSW over the survivors of every
+//                    range at once (base 2, then Lucas over the passers)
 //   k_setup_*<true>  per-prime set-up over the primes of every range at once
 //   k_batch_group_prefix  every (geometry, product) group's prefix sums of its
 //                    ranges' prime counts, in one launch
@@ -114,6 +115,9 @@ struct rs_batch {
     u64 *d_range_primes = nullptr;
     // per-range round buffers
     u64 *d_cands = nullptr, *d_primes = nullptr;
+    u64 *d_mid = nullptr;                  // base-2 probable primes of all ranges awaiting the Lucas pass
+    u32 *d_mid_r = nullptr;                //   and their ranges (R * CCAP entries)
+    u32 *d_mid_ctr = nullptr;
     PrimeHdr *d_hdr = nullptr;
     void *d_aux = nullptr;
     u64 *d_tabs = nullptr, *d_tgt = nullptr;
@@ -159,7 +163,7 @@ extern "C" void rs_batch_destroy(rs_batch *b)
     void *ptrs[] = {b->d_sp, b->d_jobs, b->d_geoms, b->d_args, b->d_fctrs, b->d_ranges, b->d_wins, b->d_ctrs,
                     b->d_range_primes, b->d_cands, b->d_primes, b->d_hdr, b->d_aux, b->d_tabs, b->d_tgt, b->d_meta,
                     b->d_err, b->d_stats, b->d_unfinished, b->d_win, b->d_prefix_c, b->d_prefix_p,
-                    b->d_gprefix, b->d_gwork};
+                    b->d_gprefix, b->d_gwork, b->d_mid, b->d_mid_r, b->d_mid_ctr};
     for (void *p : ptrs) cudaFree(p);
     if (b->h_pin) cudaFreeHost(b->h_pin);
     if (b->h_win_pin) cudaFreeHost(b->h_win_pin);
@@ -211,6 +215,8 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         !alloc((void **)&b->d_ranges, R * sizeof(BatchRange)) || !alloc((void **)&b->d_wins, R * sizeof(BatchWin)) ||
         !alloc((void **)&b->d_ctrs, (size_t)R * BR_CTRS * 4) || !alloc((void **)&b->d_range_primes, R * 8) ||
         !alloc((void **)&b->d_cands, (size_t)R * CCAP * 8) || !alloc((void **)&b->d_primes, (size_t)R * RCAP * 8) ||
+        !alloc((void **)&b->d_mid, (size_t)R * CCAP * 8) || !alloc((void **)&b->d_mid_r, (size_t)R * CCAP * 4) ||
+        !alloc((void **)&b->d_mid_ctr, 4) ||
         !alloc((void **)&b->d_hdr, (size_t)R * RCAP * sizeof(PrimeHdr)) ||
         !alloc(&b->d_aux, (size_t)R * RCAP * setup_aux_bytes()) ||
         !alloc((void **)&b->d_tabs, (size_t)R * RCAP * TABS * 8) ||
@@ -219,7 +225,7 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         !alloc((void **)&b->d_prefix_c, (R + 1) * 4) || !alloc((void **)&b->d_prefix_p, (R + 1) * 4) ||
         cudaMallocHost(&b->h_pin, 16) != cudaSuccess || cudaMallocHost(&b->h_win_pin, R * 4) != cudaSuccess) {
         rs_set_error("cannot allocate a batch of %u range slots (about %zu MB)", R,
-                     (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 10 + 24 + 8 + 16) >> 20);
+                     (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 10 + 24 + 8 + 16 + 24) >> 20);
         return fail(RS_ENOMEM);
     }
     if (cudaMemcpy(b->d_sp, sp.data(), sp.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -480,7 +486,9 @@ static int batch_round(rs_batch *b)
     BCU(launch_batch_windows(b->d_ranges, b->d_wins, b->d_win, R, RCAP, b->d_ctrs, st));
     BCU(launch_sieve_batch(b->d_wins, R, max_blocks, b->d_sp, b->nsp, b->d_cands, CCAP, b->d_ctrs, b->d_err, st));
     BCU(launch_batch_prefix_all(b->d_ranges, R, 0, CCAP, b->d_ctrs, b->d_prefix_c, st));
-    BCU(launch_mr_batch(b->d_cands, CCAP, b->d_primes, RCAP, b->d_ctrs, R, b->d_prefix_c, b->d_err, b->sms, st));
+    BCU(cudaMemsetAsync(b->d_mid_ctr, 0, 4, st));
+    BCU(launch_mr_batch2(b->d_cands, CCAP, b->d_primes, RCAP, b->d_ctrs, R, b->d_prefix_c, b->d_mid, b->d_mid_r,
+                         R * CCAP, b->d_mid_ctr, b->d_err, b->sms, st));
     BCU(launch_batch_prefix_all(b->d_ranges, R, 1, RCAP, b->d_ctrs, b->d_prefix_p, st));
     BCU(launch_setup_batch(b->d_jobs, b->d_geoms, b->d_ranges, b->d_primes, RCAP, b->d_prefix_p, R, b->d_hdr,
                            b->d_aux, b->d_tabs, b->d_tgt, b->d_meta, b->d_stats, b->d_err, b->sms, st));

@@ -30,10 +30,11 @@ struct rs_ctx {
     u32 nsp = 0;
     // segment buffers
     u64 *d_cands = nullptr;
+    u64 *d_mid = nullptr;       // base-2 strong probable primes awaiting the Lucas pass (cand_cap)
     u32 cand_cap = 0;
     u64 *d_primes = nullptr;
     u32 prime_cap = 0;
-    u32 *d_ctrs = nullptr;      // [0] sieve survivors, [1] primes, [2] BSGS work counter, [3] factor count
+    u32 *d_ctrs = nullptr;      // [0] sieve survivors, [1] primes, [2] BSGS work counter, [3] factor count, [4] mid list
     u32 *d_err = nullptr;
     u64 *d_stats = nullptr;
     u32 *h_pin = nullptr;       // pinned: ctrs[4], err
@@ -117,6 +118,7 @@ extern "C" void rs_ctx_destroy(rs_ctx *c)
     free_job(c);
     cudaFree(c->d_sp);
     cudaFree(c->d_cands);
+    cudaFree(c->d_mid);
     cudaFree(c->d_primes);
     cudaFree(c->d_ctrs);
     cudaFree(c->d_err);
@@ -162,6 +164,7 @@ extern "C" int rs_ctx_create(int device, rs_ctx **out)
     c->chunk_cap = 1u << 17;
     if (cudaMalloc(&c->d_sp, sp.size() * 4) != cudaSuccess ||
         cudaMalloc(&c->d_cands, (size_t)c->cand_cap * 8) != cudaSuccess ||
+        cudaMalloc(&c->d_mid, (size_t)c->cand_cap * 8) != cudaSuccess ||
         cudaMalloc(&c->d_primes, (size_t)c->prime_cap * 8) != cudaSuccess ||
         cudaMalloc(&c->d_ctrs, 16 * 4) != cudaSuccess || cudaMalloc(&c->d_err, 4) != cudaSuccess ||
         cudaMalloc(&c->d_stats, ST_COUNT * 8) != cudaSuccess ||
@@ -386,10 +389,11 @@ static int gen_segment(rs_ctx *c, u64 lo, u64 hi, u32 *np, bool *overflow)
     if (base >= hi) return RS_OK;
     u64 nodd = (hi - base + 1) / 2;
     CU(cudaMemsetAsync(c->d_ctrs, 0, 2 * 4, c->stream));
+    CU(cudaMemsetAsync(c->d_ctrs + 4, 0, 4, c->stream));
     CU(cudaMemsetAsync(c->d_err, 0, 4, c->stream));
     CU(launch_sieve(base, nodd, hi, c->d_sp, c->nsp, c->d_cands, c->cand_cap, c->d_ctrs, c->d_err, c->stream));
-    CU(launch_mr(c->d_cands, c->d_ctrs, c->cand_cap, c->d_primes, c->prime_cap, c->d_ctrs + 1, c->d_err, c->sms,
-                 c->stream));
+    CU(launch_mr2(c->d_cands, c->d_ctrs, c->cand_cap, c->d_primes, c->prime_cap, c->d_ctrs + 1, c->d_mid,
+                  c->d_ctrs + 4, c->d_err, c->sms, c->stream));
     CU(cudaMemcpyAsync(c->h_pin, c->d_ctrs, 2 * 4, cudaMemcpyDeviceToHost, c->stream));
     CU(cudaMemcpyAsync(c->h_pin + 4, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream));
     CU(cudaStreamSynchronize(c->stream));

@@ -1,12 +1,15 @@
 // noalloc.cu -- prime generation into caller-owned device memory, with no
 // device allocation on any call.
 //
-// The generator behind rs_primes_generate (k_sieve + k_mr of sieve.cu) needs
-// scratch: the table of odd sieving primes below 2^16, the buffer of sieve
-// survivors that k_mr tests, and two counters.  rs_primes_generate keeps
-// these in its context, allocated with cudaMalloc.  This variant keeps them in
-// one file-scope device array of fixed size, g_na_scratch below, so a call
-// allocates nothing; the caller passes the output array and the count word.
+// The generator behind rs_primes_generate (k_sieve, then the Baillie-PSW test
+// of sieve.cu) needs scratch: the table of odd sieving primes below 2^16, the
+// buffer of sieve survivors that the test reads, and counters.
+// rs_primes_generate keeps these in its context, allocated with cudaMalloc.
+// This variant keeps them in one file-scope device array of fixed size,
+// g_na_scratch below, so a call allocates nothing; the caller passes the
+// output array and the count word.  It runs the one-pass form of the test
+// (k_mr), which needs no second list of base-2 probable primes; the primes it
+// returns are the same.
 //
 // Limit: a call covers at most RS_NOALLOC_MAX_WIDTH = 2^22 integers, i.e. at
 // most 2^21 odd values, which is exactly the survivor capacity, so the

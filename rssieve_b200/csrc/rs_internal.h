@@ -197,6 +197,10 @@ cudaError_t launch_sieve(u64 base_odd, u64 nodd, u64 hi, const u32 *sp, u32 nsp,
                          u32 *ctrs, u32 *err, cudaStream_t st);
 cudaError_t launch_mr(const u64 *cands, const u32 *ctrs, u32 cand_cap, u64 *primes, u32 prime_cap, u32 *prime_ctr,
                       u32 *err, int sms, cudaStream_t st);
+// the same test in two passes (base 2 into mid, then Lucas over mid); mid
+// holds cand_cap values and *mid_ctr starts at zero
+cudaError_t launch_mr2(const u64 *cands, const u32 *ctrs, u32 cand_cap, u64 *primes, u32 prime_cap, u32 *prime_ctr,
+                       u64 *mid, u32 *mid_ctr, u32 *err, int sms, cudaStream_t st);
 cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 count, PrimeHdr *hdr, void *aux, u64 *tabs,
                          u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, int geom, cudaStream_t st);
 size_t setup_aux_bytes();
@@ -215,10 +219,13 @@ cudaError_t launch_batch_windows(BatchRange *ranges, BatchWin *wins, const u32 *
                                  cudaStream_t st);
 cudaError_t launch_sieve_batch(const BatchWin *wins, u32 nranges, u32 max_blocks, const u32 *sp, u32 nsp, u64 *cands,
                                u32 ccap, u32 *ctrs, u32 *err, cudaStream_t st);
-// Miller-Rabin over the survivors of all ranges (prefix_c: their counts'
-// prefix sums); primes go to their range's slots
-cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges,
-                            const u32 *prefix_c, u32 *err, int sms, cudaStream_t st);
+// Baillie-PSW over the survivors of all ranges (prefix_c: their counts'
+// prefix sums) in two passes: base-2 strong probable primes of every range
+// (value and range) into mid, then the Lucas test over it; primes go to their
+// range's slots; *mid_ctr starts at zero
+cudaError_t launch_mr_batch2(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges,
+                             const u32 *prefix_c, u64 *mid, u32 *mid_r, u32 mid_cap, u32 *mid_ctr, u32 *err, int sms,
+                             cudaStream_t st);
 // set-up of the primes of all ranges (prefix_p: prefix sums of their counts)
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
                                u32 rcap, const u32 *prefix_p, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs,

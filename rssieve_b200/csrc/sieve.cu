@@ -191,11 +191,17 @@ __device__ __forceinline__ u64 mhalf(u64 x, u64 n)
 // Strong Lucas probable-prime test with Selfridge's parameters: D is the first
 // of 5, -7, 9, -11, ... with Jacobi (D/n) = -1, P = 1, Q = (1 - D)/4; with
 // n + 1 = d * 2^s (d odd), n passes if U_d = 0 or V_(d*2^r) = 0 for some r < s.
-// U, V and Q^k run in Montgomery form through the doubling formulas
-// U_2k = U_k V_k, V_2k = V_k^2 - 2Q^k and the step k -> k+1 (U' = (U + V)/2,
-// V' = (D U + V)/2).  Returns 1 (probable prime), 0 (composite), or -1 when no
-// D turned up within 64 candidates (the caller then decides otherwise).
-// n is odd, above 65537^2 and below 2^64 - 1.
+// Only V is carried: the ladder keeps the pair (V_k, V_(k+1)) and Q^k in
+// Montgomery form and per bit b of d forms
+//   V_(2k+1) = V_k V_(k+1) - P Q^k,   V_(2(k+b)) = V_(k+b)^2 - 2 Q^(k+b),
+//   Q^(2k+b) = Q^k Q^(k+b),
+// four products whatever b is, so the lanes of a warp never diverge on the
+// bits of their own d.  U_d follows from D U_k = 2 V_(k+1) - P V_k (with
+// alpha, beta the roots of x^2 - P x + Q: 2(alpha^(k+1) + beta^(k+1)) -
+// (alpha + beta)(alpha^k + beta^k) = (alpha - beta)(alpha^k - beta^k)), and
+// gcd(D, n) = 1, so U_d = 0 exactly when 2 V_(d+1) = V_d.  Returns 1 (probable
+// prime), 0 (composite), or -1 when no D turned up within 64 candidates (the
+// caller then decides otherwise).  n is odd, above 65537^2 and below 2^64 - 1.
 __device__ int lucas_strong(u64 n, const Mont &M)
 {
     int D = 5;
@@ -212,25 +218,22 @@ __device__ int lucas_strong(u64 n, const Mont &M)
     }
     const int Qi = (1 - D) / 4;
     const u64 Qm = to_mont(Qi >= 0 ? (u64)Qi : n - (u64)(-Qi), M);
-    const u64 Dm = to_mont(D >= 0 ? (u64)D : n - (u64)(-D), M);
     const int s = __ffsll((long long)(n + 1)) - 1;
     const u64 d = (n + 1) >> s;
-    u64 U = M.one, V = M.one, Qk = Qm;                     // k = 1: U_1 = 1, V_1 = P = 1
+    // k = 1: V_1 = P = 1, V_2 = P^2 - 2Q
+    u64 Vk = M.one, Vk1 = msub(M.one, madd(Qm, Qm, n), n), Qk = Qm;
     for (int bit = 62 - __clzll(d); bit >= 0; --bit) {
-        const u64 U2 = mmul(U, V, n, M.q);
-        const u64 V2 = msub(mmul(V, V, n, M.q), madd(Qk, Qk, n), n);
-        const u64 Qk2 = mmul(Qk, Qk, n, M.q);
-        if ((d >> bit) & 1) {
-            U = mhalf(madd(U2, V2, n), n);
-            V = mhalf(madd(mmul(Dm, U2, n, M.q), V2, n), n);
-            Qk = mmul(Qk2, Qm, n, M.q);
-        } else {
-            U = U2;
-            V = V2;
-            Qk = Qk2;
-        }
+        const bool one = (d >> bit) & 1;
+        const u64 t = mmul(Qk, one ? Qm : M.one, n, M.q);            // Q^(k+b)
+        const u64 mid = msub(mmul(Vk, Vk1, n, M.q), Qk, n);          // V_(2k+1)
+        const u64 vs = one ? Vk1 : Vk;
+        const u64 sq = msub(mmul(vs, vs, n, M.q), madd(t, t, n), n);  // V_(2(k+b))
+        Qk = mmul(Qk, t, n, M.q);
+        Vk = one ? mid : sq;
+        Vk1 = one ? sq : mid;
     }
-    if (U == 0) return 1;
+    if (madd(Vk1, Vk1, n) == Vk) return 1;                 // U_d = 0
+    u64 V = Vk;
     for (int r = 0; r < s; ++r) {
         if (V == 0) return 1;
         if (r + 1 < s) {
@@ -239,6 +242,26 @@ __device__ int lucas_strong(u64 n, const Mont &M)
         }
     }
     return 0;
+}
+
+// Strong probable prime to base 2: 2^d by squarings with a doubling (an
+// addition) for every set bit of d below the top one, chosen by select so the
+// lanes of a warp stay converged.
+__device__ __forceinline__ bool sprp2(u64 n, const Mont &M, u64 d, int t)
+{
+    const u64 mone = n - M.one;
+    u64 x = madd(M.one, M.one, n);                         // 2 in Montgomery form
+    for (int bit = 62 - __clzll(d); bit >= 0; --bit) {
+        x = mmul(x, x, n, M.q);
+        const u64 x2 = madd(x, x, n);
+        x = ((d >> bit) & 1) ? x2 : x;
+    }
+    if (x == M.one || x == mone) return true;
+    for (int i = 1; i < t; ++i) {
+        x = mmul(x, x, n, M.q);
+        if (x == mone) return true;
+    }
+    return false;
 }
 
 // Deterministic primality of a sieve survivor below 2^64 (Baillie-PSW): a
@@ -258,12 +281,31 @@ __device__ bool is_prime_bpsw(u64 n)
     const Mont M = mont_init(n);
     const u64 nm1 = n - 1;
     const int t = __ffsll((long long)nm1) - 1;
-    if (!sprp_base(n, M, nm1 >> t, t, 2)) return false;
+    if (!sprp2(n, M, nm1 >> t, t)) return false;
     const int l = lucas_strong(n, M);
     return (l >= 0) ? (l == 1) : is_prime_mr(n);
 }
 
-// Warp-stride Miller-Rabin over cands[0, min(*cand_ctr, cand_cap)) with ballot compaction into primes.
+// Appends v of the lanes with keep set to list[*ctr ...] with one atomic per
+// warp (ballot compaction); flags err and drops the warp's values when the
+// list is full.  All 32 lanes call it.
+__device__ __forceinline__ void warp_push(bool keep, u64 v, u64 *__restrict__ list, u32 cap, u32 *ctr, u32 *err,
+                                          u32 flag)
+{
+    const u32 lane = threadIdx.x & 31;
+    const u32 mask = __ballot_sync(0xFFFFFFFFu, keep);
+    if (!mask) return;
+    u32 basepos = 0;
+    if (lane == 0) basepos = atomicAdd(ctr, __popc(mask));
+    basepos = __shfl_sync(0xFFFFFFFFu, basepos, 0);
+    if (basepos + __popc(mask) > cap) {
+        if (lane == 0) atomicOr(err, flag);
+        return;
+    }
+    if (keep) list[basepos + __popc(mask & ((1u << lane) - 1))] = v;
+}
+
+// Warp-stride Baillie-PSW over cands[0, min(*cand_ctr, cand_cap)) with ballot compaction into primes.
 __device__ __forceinline__ void mr_list(const u64 *__restrict__ cands, const u32 *cand_ctr, u32 cand_cap,
                                         u64 *__restrict__ primes, u32 prime_cap, u32 *prime_ctr, u32 *err)
 {
@@ -272,23 +314,14 @@ __device__ __forceinline__ void mr_list(const u64 *__restrict__ cands, const u32
     const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
     for (u32 b0 = warp * 32; b0 < n; b0 += nwarps * 32) {
-        u32 idx = b0 + lane;
+        const u32 idx = b0 + lane;
         u64 v = 0;
         bool pr = false;
         if (idx < n) {
             v = cands[idx];
             pr = is_prime_bpsw(v);
         }
-        u32 mask = __ballot_sync(0xFFFFFFFFu, pr);
-        if (!mask) continue;
-        u32 basepos = 0;
-        if (lane == 0) basepos = atomicAdd(prime_ctr, __popc(mask));
-        basepos = __shfl_sync(0xFFFFFFFFu, basepos, 0);
-        if (basepos + __popc(mask) > prime_cap) {
-            if (lane == 0) atomicOr(err, ERR_PRIME_OVERFLOW);
-            continue;
-        }
-        if (pr) primes[basepos + __popc(mask & ((1u << lane) - 1))] = v;
+        warp_push(pr, v, primes, prime_cap, prime_ctr, err, ERR_PRIME_OVERFLOW);
     }
 }
 
@@ -299,18 +332,121 @@ __global__ void __launch_bounds__(256) k_mr(const u64 *__restrict__ cands, const
     mr_list(cands, ctrs, cand_cap, primes, prime_cap, prime_ctr, err);
 }
 
-// Batch round: the survivors of every range as one index space (prefix_c:
-// prefix sums of their counts), so a few active ranges still fill the device;
-// each prime takes a slot of its range with one atomic.
-__global__ void __launch_bounds__(256) k_mr_batch(const u64 *__restrict__ cands, u32 ccap, u64 *__restrict__ primes,
-                                                  u32 rcap, u32 *ctrs, const u32 *__restrict__ prefix_c, u32 nr,
-                                                  u32 *err)
+// The same test in two passes, so that the Lucas ladder runs on full warps.
+// About 57% of the survivors of a sieve by the primes below 2^16 are prime at
+// p near 2^50 (Mertens: 1/ln p over e^-gamma/ln 2^16), and the base-2 test
+// rejects almost every composite; in one pass a warp runs the Lucas ladder
+// (four products per bit, against about one for the base-2 test) as soon as
+// one lane passed base 2, so 40% of its lanes idle through it.  Pass 1 sends
+// survivors below 65537^2 (proven by the sieve) to primes and base-2 strong
+// probable primes to mid; pass 2 runs the Lucas test over mid.
+__global__ void __launch_bounds__(256) k_mr_sprp(const u64 *__restrict__ cands, const u32 *__restrict__ ctrs,
+                                                 u32 cand_cap, u64 *__restrict__ primes, u32 prime_cap,
+                                                 u32 *prime_ctr, u64 *__restrict__ mid, u32 *mid_ctr, u32 *err)
+{
+    const u32 n = min(ctrs[0], cand_cap);
+    const u32 lane = threadIdx.x & 31;
+    const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 b0 = warp * 32; b0 < n; b0 += nwarps * 32) {
+        const u32 idx = b0 + lane;
+        u64 v = 0;
+        bool small = false, pass = false;
+        if (idx < n) {
+            v = cands[idx];
+            if (v < MR_BOUND) {
+                small = true;
+            } else if (v != ~0ull) {       // 2^64 - 1 = 3 * 5 * 17 * 257 * 641 * 65537 * 6700417
+                const Mont M = mont_init(v);
+                const int t = __ffsll((long long)(v - 1)) - 1;
+                pass = sprp2(v, M, (v - 1) >> t, t);
+            }
+        }
+        warp_push(small, v, primes, prime_cap, prime_ctr, err, ERR_PRIME_OVERFLOW);
+        warp_push(pass, v, mid, cand_cap, mid_ctr, err, ERR_CAND_OVERFLOW);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_mr_lucas(const u64 *__restrict__ mid, const u32 *__restrict__ mid_ctr,
+                                                  u32 mid_cap, u64 *__restrict__ primes, u32 prime_cap,
+                                                  u32 *prime_ctr, u32 *err)
+{
+    const u32 n = min(*mid_ctr, mid_cap);
+    const u32 lane = threadIdx.x & 31;
+    const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 b0 = warp * 32; b0 < n; b0 += nwarps * 32) {
+        const u32 idx = b0 + lane;
+        u64 v = 0;
+        bool pr = false;
+        if (idx < n) {
+            v = mid[idx];
+            const int l = lucas_strong(v, mont_init(v));
+            pr = (l >= 0) ? (l == 1) : is_prime_mr(v);
+        }
+        warp_push(pr, v, primes, prime_cap, prime_ctr, err, ERR_PRIME_OVERFLOW);
+    }
+}
+
+// Batch round in two passes, as k_mr_sprp/k_mr_lucas: pass 1 over the
+// survivors of every range (one index space, prefix_c) sends the base-2 strong
+// probable primes, with their range, to one mid list; pass 2 runs the Lucas
+// test over it.  Survivors below 65537^2 go straight to their range's slots.
+__global__ void __launch_bounds__(256) k_mr_batch_sprp(const u64 *__restrict__ cands, u32 ccap,
+                                                       u64 *__restrict__ primes, u32 rcap, u32 *ctrs,
+                                                       const u32 *__restrict__ prefix_c, u32 nr,
+                                                       u64 *__restrict__ mid, u32 *__restrict__ mid_r, u32 mid_cap,
+                                                       u32 *mid_ctr, u32 *err)
 {
     const u32 total = prefix_c[nr];
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        const u32 r = prefix_find(prefix_c, nr, i);
-        const u64 v = cands[(size_t)r * ccap + (i - prefix_c[r])];
-        if (!is_prime_bpsw(v)) continue;
+    const u32 lane = threadIdx.x & 31;
+    const u32 warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const u32 nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 b0 = warp * 32; b0 < total; b0 += nwarps * 32) {
+        const u32 i = b0 + lane;
+        u64 v = 0;
+        u32 r = 0;
+        bool pass = false;
+        if (i < total) {
+            r = prefix_find(prefix_c, nr, i);
+            v = cands[(size_t)r * ccap + (i - prefix_c[r])];
+            if (v < MR_BOUND) {
+                const u32 pos = atomicAdd(&ctrs[r * BR_CTRS + 1], 1u);
+                if (pos < rcap) primes[(size_t)r * rcap + pos] = v;
+                else atomicOr(err, ERR_PRIME_OVERFLOW);
+            } else if (v != ~0ull) {
+                const Mont M = mont_init(v);
+                const int t = __ffsll((long long)(v - 1)) - 1;
+                pass = sprp2(v, M, (v - 1) >> t, t);
+            }
+        }
+        const u32 mask = __ballot_sync(0xFFFFFFFFu, pass);
+        if (!mask) continue;
+        u32 basepos = 0;
+        if (lane == 0) basepos = atomicAdd(mid_ctr, __popc(mask));
+        basepos = __shfl_sync(0xFFFFFFFFu, basepos, 0);
+        if (basepos + __popc(mask) > mid_cap) {
+            if (lane == 0) atomicOr(err, ERR_CAND_OVERFLOW);
+            continue;
+        }
+        if (pass) {
+            const u32 pos = basepos + __popc(mask & ((1u << lane) - 1));
+            mid[pos] = v;
+            mid_r[pos] = r;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_mr_batch_lucas(const u64 *__restrict__ mid, const u32 *__restrict__ mid_r,
+                                                        u32 mid_cap, const u32 *__restrict__ mid_ctr,
+                                                        u64 *__restrict__ primes, u32 rcap, u32 *ctrs, u32 *err)
+{
+    const u32 n = min(*mid_ctr, mid_cap);
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const u64 v = mid[i];
+        const int l = lucas_strong(v, mont_init(v));
+        if (!((l >= 0) ? (l == 1) : is_prime_mr(v))) continue;
+        const u32 r = mid_r[i];
         const u32 pos = atomicAdd(&ctrs[r * BR_CTRS + 1], 1u);
         if (pos < rcap) primes[(size_t)r * rcap + pos] = v;
         else atomicOr(err, ERR_PRIME_OVERFLOW);
@@ -369,10 +505,13 @@ cudaError_t launch_sieve_batch(const BatchWin *wins, u32 nranges, u32 max_blocks
     return cudaGetLastError();
 }
 
-cudaError_t launch_mr_batch(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges,
-                            const u32 *prefix_c, u32 *err, int sms, cudaStream_t st)
+cudaError_t launch_mr_batch2(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges,
+                             const u32 *prefix_c, u64 *mid, u32 *mid_r, u32 mid_cap, u32 *mid_ctr, u32 *err, int sms,
+                             cudaStream_t st)
 {
-    k_mr_batch<<<sms * 8, 256, 0, st>>>(cands, ccap, primes, rcap, ctrs, prefix_c, nranges, err);
+    k_mr_batch_sprp<<<sms * 8, 256, 0, st>>>(cands, ccap, primes, rcap, ctrs, prefix_c, nranges, mid, mid_r, mid_cap,
+                                              mid_ctr, err);
+    k_mr_batch_lucas<<<sms * 8, 256, 0, st>>>(mid, mid_r, mid_cap, mid_ctr, primes, rcap, ctrs, err);
     return cudaGetLastError();
 }
 
@@ -380,6 +519,14 @@ cudaError_t launch_mr(const u64 *cands, const u32 *ctrs, u32 cand_cap, u64 *prim
                       u32 *err, int sms, cudaStream_t st)
 {
     k_mr<<<sms * 8, 256, 0, st>>>(cands, ctrs, cand_cap, primes, prime_cap, prime_ctr, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mr2(const u64 *cands, const u32 *ctrs, u32 cand_cap, u64 *primes, u32 prime_cap, u32 *prime_ctr,
+                       u64 *mid, u32 *mid_ctr, u32 *err, int sms, cudaStream_t st)
+{
+    k_mr_sprp<<<sms * 8, 256, 0, st>>>(cands, ctrs, cand_cap, primes, prime_cap, prime_ctr, mid, mid_ctr, err);
+    k_mr_lucas<<<sms * 8, 256, 0, st>>>(mid, mid_ctr, cand_cap, primes, prime_cap, prime_ctr, err);
     return cudaGetLastError();
 }
 
