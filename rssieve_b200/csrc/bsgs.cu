@@ -182,6 +182,7 @@ struct PrimeCtx {
     u64 p, q, s;         // the prime, p^-1 mod 2^64, Montgomery b^e
     u32 smul, e;         // baby-step multiplier when additions suffice; split modulus
     u32 cp, qp;          // baby steps per thread and per prime (qp = TPB * cp)
+    u32 fp;              // FP64 steps (MODE 2): table and giant values are the bits of doubles
 };
 extern __shared__ __align__(128) unsigned char smem_raw[];
 __shared__ BsgsArgs s_args;
@@ -190,6 +191,14 @@ __shared__ PrimeCtx s_ctx;
 __shared__ unsigned long long s_cands, s_dups, s_facs;   // per-CTA totals
 __shared__ unsigned long long s_baby, s_giant, s_small;  // per-CTA totals kept by thread 0
 __shared__ u32 s_nsol, s_sol_i[KMAX], s_sol_u0[KMAX];   // small-order solutions
+
+// A residue's table value: the residue itself, or with FP64 steps (MODE 2) the
+// bit pattern of the double that holds it exactly (every step of that mode
+// yields canonical residues, so equal residues have equal bits).
+__device__ __forceinline__ u64 fp_val(u64 v) { return (u64)__double_as_longlong((double)v); }
+__device__ __forceinline__ u64 fp_res(u64 bits) { return (u64)__longlong_as_double((long long)bits); }
+__device__ __forceinline__ u64 to_val(u64 v) { return s_ctx.fp ? fp_val(v) : v; }
+__device__ __forceinline__ u64 to_res(u64 val) { return s_ctx.fp ? fp_res(val) : val; }
 
 // Dynamic shared memory: fingerprints | indices | counts | start values | giant
 // start powers | two record staging buffers.
@@ -232,14 +241,15 @@ __device__ __forceinline__ void claim(u64 p, u32 seq, u32 n)
     }
 }
 
-// exact check of a fingerprint match: y_j == val ?  (y_j from its thread's start)
+// exact check of a fingerprint match: y_j == val ?  (y_j from its thread's
+// start, by integer steps on the residues whatever the launch's step kind)
 __device__ __forceinline__ bool verify(const u64 *s_start, u32 j, u64 val)
 {
     const PrimeCtx c = s_ctx;
     if (j >= c.qp) return false;
-    u64 y = s_start[j / c.cp];
+    u64 y = to_res(s_start[j / c.cp]);
     for (u32 r = j % c.cp; r; --r) y = baby_step(y, c.smul, c.s, c.p, c.q);
-    return y == val;
+    return y == to_res(val);
 }
 
 // Giant-step match or overflowed bucket: check every matching slot of the
@@ -319,13 +329,13 @@ __device__ __noinline__ void rebuild_table(u32 order)
     const PrimeCtx c = s_ctx;
     clear_table(T, NB);
     __syncthreads();
-    u64 y = st[threadIdx.x];
+    u64 y = to_res(st[threadIdx.x]);
     u32 pend = 0;
     for (u32 i = 0; i < c.cp; ++i) {
         const u32 j = threadIdx.x * c.cp + i;
         if (j < order) {
             u32 b, fpv;
-            tab_hash<NB>(y, b, fpv);
+            tab_hash<NB>(to_val(y), b, fpv);
             int pr = 0;
             while (pr < BSGS_MAXPROBE && !tab_try<NB>(T, b, fpv, j)) ++pr;
             if (pr >= BSGS_MAXPROBE) pend = 1;
@@ -346,7 +356,7 @@ __device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
     const u64 *st = Smem<TPB, NB>::start();
     const u32 tid = threadIdx.x;
     if (tid < R->hdr.numk) {
-        const u64 Tv = R->tgt[tid];
+        const u64 Tv = to_val(R->tgt[tid]);
         u32 b, fp;
         tab_hash<NB>(Tv, b, fp);
         for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
@@ -387,7 +397,8 @@ __device__ __forceinline__ u32 batch_slot(u32 i, u32 nr, const u32 *prefix, u32 
     return k * rcap + (i - prefix[k]);
 }
 
-// MODE: 1 = every prime below 2^63 (Shoup giant steps), 0 = every prime at or
+// MODE: 2 = every prime below FP_BOUND = 2^51 (FP64 baby and giant steps,
+// fp_mulfix), 1 = every prime below 2^63 (Shoup steps), 0 = every prime at or
 // above 2^63 (Montgomery giant steps).  1024 / TPB CTAs share an SM, so the
 // bound keeps each thread at 64 registers.  BATCH: the primes of several
 // ranges (jobs) in one launch -- work item i maps to a record slot through the
@@ -480,7 +491,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             s_nsol = 0;
             s_spill = 0;
             s_ctx.p = p; s_ctx.q = q; s_ctx.s = s; s_ctx.smul = smul; s_ctx.e = e;
-            s_ctx.cp = cp; s_ctx.qp = TPB * cp;
+            s_ctx.cp = cp; s_ctx.qp = TPB * cp; s_ctx.fp = (MODE == 2);
             if (BATCH) s_args = s_args_next;
         }
         if (live) clear_table(T, NB);
@@ -499,9 +510,10 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             // ---- baby steps y_j = s^j, j < Q' = TPB*cp, inserted as they are produced ----
             // Speculative: ord(s) < Q' is only known after the barrier; then the
             // table (which may hold repeats) is rebuilt from j < ord.
-            const u64 one = R.hdr.one;
             const u64 x0 = mmul(R.tabs[tid & 31], R.tabs[32 + (tid >> 5)], p, q);   // s^(cp*tid)
-            s_start[tid] = x0;
+            // MODE 2: table values are the bits of the doubles holding the residues
+            const u64 one = (MODE == 2) ? fp_val(R.hdr.one) : R.hdr.one;
+            s_start[tid] = (MODE == 2) ? fp_val(x0) : x0;
             u32 spill = 0;
             // Two chains per thread, j in [tid*cp, tid*cp + cp/2) and the next
             // cp/2 (started from s^(cp/2) further), so the two products of a step
@@ -516,12 +528,20 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             const u64 sp = R.hdr.sp;
             const u32 half = cp >> 1;
             u64 xa = x0, xb = mmul(x0, R.hdr.u2, p, q);
+            if (MODE == 2) { xa = fp_val(xa); xb = fp_val(xb); }
+            const double pd = (double)p, sd = (double)sp, sq = __longlong_as_double((long long)R.hdr.S);
             // IB2 values of each chain are hashed and stepped, then inserted, per
             // round (IB2 = IBMAX/2, or cp/2 when it is smaller)
             auto babies = [&](auto kind, auto ibc) {
                 constexpr int K = decltype(kind)::value;          // 2, 4: doublings; 1: Shoup; 0: baby_step
                 constexpr int IB2 = decltype(ibc)::value;
                 auto step = [&](u64 v) -> u64 {
+                    if (MODE == 2) {
+                        double x = __longlong_as_double((long long)v);
+                        if (K == 1) x = fp_mulfix(x, sd, sq, pd);
+                        else { x = fp_dbl(x, pd); if (K == 4) x = fp_dbl(x, pd); }
+                        return (u64)__double_as_longlong(x);
+                    }
                     if (K == 0) return baby_step(v, smul, s, p, q);
                     if (K == 1) return shoup_mul(v, sp, ssw, p);
                     if (MODE == 1) { v = dbl63(v, p); return (K == 4) ? dbl63(v, p) : v; }
@@ -554,14 +574,16 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                     }
                 }
             };
+            // (FP64 steps keep three double constants live: rounds of two
+            // values per chain keep the loop within 64 registers)
             auto babies_cp = [&](auto kind) {
-                if (half >= IBMAX / 2) babies(kind, std::integral_constant<int, IBMAX / 2>{});
+                if (MODE != 2 && half >= IBMAX / 2) babies(kind, std::integral_constant<int, IBMAX / 2>{});
                 else if (half >= IBMAX / 4) babies(kind, std::integral_constant<int, IBMAX / 4>{});
                 else babies(kind, std::integral_constant<int, IBMAX / 8>{});
             };
             if (smul == 2) babies_cp(std::integral_constant<int, 2>{});
             else if (smul == 4) babies_cp(std::integral_constant<int, 4>{});
-            else if constexpr (MODE == 1) babies_cp(std::integral_constant<int, 1>{});
+            else if constexpr (MODE >= 1) babies_cp(std::integral_constant<int, 1>{});
             else babies_cp(std::integral_constant<int, 0>{});
             if (minj != 0xFFFFFFFFu) atomicMin(&s_order, minj);
             if (spill) s_spill = 1;
@@ -590,6 +612,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                 // quotient constant), else the Montgomery product by S.
                 const u32 numk = R.hdr.numk, G = R.hdr.G, Lc = R.hdr.Lc;
                 const u64 S = R.hdr.S, Sw = R.hdr.Sw, Sp = R.hdr.Sp;
+                const double pd = (double)p, Sd = (double)Sp, Sqd = __longlong_as_double((long long)R.hdr.Sq);
                 if (tid < numk * G) {
                     const u32 i = tid / G, g = tid - i * G;
                     const u32 q0 = g * Lc;
@@ -599,24 +622,26 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                     const u32 m = R.meta[i];
                     u64 gA = mmul(R.tgt[i], s_Z[g], p, q);
                     u64 gB = mmul(gA, R.hdr.Sh, p, q);
-                    auto walk = [&](auto shoup) {
-                        constexpr bool SH = decltype(shoup)::value;
-                        // chain B has nA or nA+1 steps, except in a target's last,
-                        // shorter chunk, where it may have fewer or none
-                        const u32 nt = max(nA, nB);
-                        for (u32 t = 0; t < nt; ++t) {
-                            if (t < nA) {
-                                giant_probe<TPB, C, NB>(T, gA, q0 + t, m);
-                                gA = SH ? shoup_mul(gA, Sp, Sw, p) : mmul(gA, S, p, q);
-                            }
-                            if (t < nB) {
-                                giant_probe<TPB, C, NB>(T, gB, q0 + h + t, m);
-                                gB = SH ? shoup_mul(gB, Sp, Sw, p) : mmul(gB, S, p, q);
-                            }
-                        }
+                    if (MODE == 2) { gA = fp_val(gA); gB = fp_val(gB); }
+                    auto gstep = [&](u64 v) -> u64 {
+                        if (MODE == 2)
+                            return (u64)__double_as_longlong(fp_mulfix(__longlong_as_double((long long)v), Sd, Sqd, pd));
+                        if (MODE == 1) return shoup_mul(v, Sp, Sw, p);
+                        return mmul(v, S, p, q);
                     };
-                    if (MODE == 1) walk(std::true_type{});
-                    else walk(std::false_type{});
+                    // chain B has nA or nA+1 steps, except in a target's last,
+                    // shorter chunk, where it may have fewer or none
+                    const u32 nt = max(nA, nB);
+                    for (u32 t = 0; t < nt; ++t) {
+                        if (t < nA) {
+                            giant_probe<TPB, C, NB>(T, gA, q0 + t, m);
+                            gA = gstep(gA);
+                        }
+                        if (t < nB) {
+                            giant_probe<TPB, C, NB>(T, gB, q0 + h + t, m);
+                            gB = gstep(gB);
+                        }
+                    }
                 }
             } else {
                 small_order_search<TPB, C, NB>(&R, order);
@@ -702,11 +727,11 @@ cudaError_t bsgs_prepare()
 {
     cudaError_t e = cudaSuccess;
     auto chk = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
-    chk(set_smem<0, 0>()); chk(set_smem<0, 1>());
-    chk(set_smem<1, 0>()); chk(set_smem<1, 1>());
-    chk(set_smem<2, 0>()); chk(set_smem<2, 1>());
-    chk(set_smem<3, 0>()); chk(set_smem<3, 1>());
-    chk(set_smem<4, 0>()); chk(set_smem<4, 1>());
+    chk(set_smem<0, 0>()); chk(set_smem<0, 1>()); chk(set_smem<0, 2>());
+    chk(set_smem<1, 0>()); chk(set_smem<1, 1>()); chk(set_smem<1, 2>());
+    chk(set_smem<2, 0>()); chk(set_smem<2, 1>()); chk(set_smem<2, 2>());
+    chk(set_smem<3, 0>()); chk(set_smem<3, 1>()); chk(set_smem<3, 2>());
+    chk(set_smem<4, 0>()); chk(set_smem<4, 1>()); chk(set_smem<4, 2>());
     return e;
 }
 
@@ -717,11 +742,13 @@ cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs,
     if (count == 0) return cudaSuccess;
     const u64 TOP = 1ull << 63;
     if (pmin < TOP && pmax > TOP) return cudaErrorInvalidValue;   // the caller splits launches at 2^63
-    const bool shoup = (pmax <= TOP);
+    if (pmin < FP_BOUND && pmax > FP_BOUND) return cudaErrorInvalidValue;   // and at FP_BOUND
+    const int mode = (pmax <= FP_BOUND) ? 2 : (pmax <= TOP) ? 1 : 0;
 #define RS_BSGS_CASE(G)                                                                                  \
     case G:                                                                                              \
-        return shoup ? launch_geom<G, 1>(a, hdr, tabs, tgt, meta, count, work_ctr, sms, st)              \
-                     : launch_geom<G, 0>(a, hdr, tabs, tgt, meta, count, work_ctr, sms, st);
+        return mode == 2 ? launch_geom<G, 2>(a, hdr, tabs, tgt, meta, count, work_ctr, sms, st)          \
+             : mode == 1 ? launch_geom<G, 1>(a, hdr, tabs, tgt, meta, count, work_ctr, sms, st)          \
+                         : launch_geom<G, 0>(a, hdr, tabs, tgt, meta, count, work_ctr, sms, st);
     switch (geom) {
         RS_BSGS_CASE(0)
         RS_BSGS_CASE(1)

@@ -485,6 +485,7 @@ extern "C" int rs_run_range(rs_ctx *c, uint64_t p0, uint64_t p1, rs_counters *de
     while (p < p1) {
         u64 hi = (p1 - p > width) ? p + width : p1;
         if (p < TOP && hi > TOP) hi = TOP;          // a launch is either all Shoup or all Montgomery
+        if (p < FP_BOUND && hi > FP_BOUND) hi = FP_BOUND;   // and either all FP64 or all integer steps
         rc = ensure_events(c, 2);
         if (rc) return rc;
         CU(cudaEventRecord(c->ev[0], c->stream));

@@ -110,12 +110,18 @@ struct JobDev {
     u32 *bitmap;         // kcount * words
 };
 
+// Below FP_BOUND = 2^51 the BSGS steps run on the FP64 pipe (fp_mulfix in
+// mont.cuh): residues are exact integers in doubles, and a product by a fixed
+// multiplier w takes its quotient from the double w/p.
+constexpr u64 FP_BOUND = 1ull << 51;
+
 struct PrimeHdr {        // 128 bytes (a 16-byte multiple: copied by TMA bulk copies)
     u64 p;               // 0 = skipped
     u64 q;               // p^-1 mod 2^64
     u64 one;             // 2^64 mod p
     u64 s;               // Montgomery b^e, e = the split modulus (n runs over one class mod e per target)
-    u64 S;               // Montgomery s^Q' (Q' = this prime's baby-step count)
+    u64 S;               // Montgomery s^Q' (Q' = this prime's baby-step count), for p >= 2^63; below
+                         // FP_BOUND the bits of the double sp/p (FP64 baby steps)
     u32 numk;            // surviving targets
     u32 e;               // split modulus, 1..64
     u32 G, Lc;           // giant phase: G chunks of Lc giant steps
@@ -128,7 +134,7 @@ struct PrimeHdr {        // 128 bytes (a 16-byte multiple: copied by TMA bulk co
     u64 ssw;             // floor(sp*2^64/p), sp = s mod p (plain), for Shoup baby steps; 0 when p >= 2^63
     u64 sp, Sp;          // s and s^Q' as plain residues, the Shoup multipliers (0 when p >= 2^63)
     u64 u2;              // Montgomery s^(cp/2): start offset of a thread's second baby chain
-    u64 pad2_;
+    u64 Sq;              // below FP_BOUND: the bits of the double Sp/p (FP64 giant steps); else 0
 };
 static_assert(sizeof(PrimeHdr) == 128, "PrimeHdr is copied in 16-byte units");
 

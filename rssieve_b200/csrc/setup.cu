@@ -108,7 +108,7 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
 {
     PrimeHdr H;
     H.p = 0; H.q = 0; H.one = 0; H.s = 0; H.S = 0; H.numk = 0; H.e = 0; H.G = 0; H.Lc = 0; H.smul = 0; H.job = jb;
-    H.Mg = 0; H.cp = 0; H.Sh = 0; H.Sw = 0; H.ssw = 0; H.sp = 0; H.Sp = 0; H.u2 = 0; H.pad2_ = 0;
+    H.Mg = 0; H.cp = 0; H.Sh = 0; H.Sw = 0; H.ssw = 0; H.sp = 0; H.Sp = 0; H.u2 = 0; H.Sq = 0;
     const Mont M = mont_init(p);
     const u32 b = job->base;
     const u64 bm = to_mont(b, M);
@@ -428,6 +428,11 @@ __device__ __forceinline__ void setup_tabs_one(const JobDev *__restrict__ job, u
     if (!(p >> 63)) {                                      // Shoup multiplier of the giant steps below 2^63
         h.Sp = from_mont(S, M);
         h.Sw = shoup_of_mont(S, q);
+    }
+    if (p < FP_BOUND) {                                    // FP64 quotients of the baby and giant multipliers
+        const double pd = (double)p;
+        h.S = (u64)__double_as_longlong((double)H.sp / pd);
+        h.Sq = (u64)__double_as_longlong((double)h.Sp / pd);
     }
     n_targets += nk;
     if (e >= 2) ++n_split; else ++n_full;

@@ -100,6 +100,26 @@ def test_config2_job_planted_at_2_50(sieve, oracle, rs):
     assert all((s, n) in got for s, n, _ in planted)
 
 
+def test_config2_job_planted_across_2_51_and_at_2_62(sieve, oracle, rs):
+    """The config-2 job with sequences re-drawn so that primes on both sides of
+    2^51 (the engine splits the window there: FP64 baby and giant steps below,
+    Shoup steps above) and primes of a window at 2^62 (Shoup steps; k < 2^40
+    there, so that small enough k exist) divide candidate terms."""
+    mid = 1 << 51
+    job, lo = plant_job(oracle, W.config2(2), mid - 4096, mid, 6, 1 << 32, 1, seqs=list(range(2, 100, 8)))
+    job, hi = plant_job(oracle, job, mid, mid + 4096, 6, 1 << 32, 1, seqs=list(range(6, 100, 8)))
+    assert len(lo) >= 4 and len(hi) >= 4
+    fac = _check_single(sieve, oracle, rs, job, mid - 4096, mid + 4096, len(lo) + len(hi))
+    got = _terms(fac)
+    assert all((s, n) in got for s, n, _ in lo + hi)
+    p0 = 1 << 62
+    job, planted = plant_job(oracle, W.config2(2), p0, p0 + 8192, 8, 1 << 40, 1, seqs=list(range(2, 100, 8)))
+    assert len(planted) >= 6
+    fac = _check_single(sieve, oracle, rs, job, p0, p0 + 8192, len(planted))
+    got = _terms(fac)
+    assert all((s, n) in got for s, n, _ in planted)
+
+
 def test_config4_job_planted_near_2_64(sieve, oracle, rs):
     """The config-4 job (b = 5, 20 sequences, k even < 2^40, c alternating) with
     sequences re-drawn so that primes of the first 2^16 of its p-range, just
