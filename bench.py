@@ -483,6 +483,7 @@ def main():
     sv.set_stream(stream.cuda_stream)
     peak = sv.mulmod_peak()
     wide = sv.widemul_peak()
+    fpeak = sv.fpmul_peak()
     sms = torch.cuda.get_device_properties(local).multi_processor_count
     sv.set_baby_steps(args.baby_steps)
     sv.load(seqs)
@@ -532,6 +533,10 @@ def main():
     # table insert or probe each) / average launch time
     achieved = ((tot["giant"] + tot["baby"]) / max(bsgs_launches, 1)) / (bsgs_ms_avg / 1e3) / 1e9
     peak_mult = wide / 11.0                       # products the 32x32->64 multiplier allows
+    # below 2^51 the steps' products run on the FP64 pipe: the roofline is then
+    # the FP64 product rate; above, the Montgomery-product rate
+    fp_steps = p_start + nwin * world * width <= (1 << 51)
+    rpeak = fpeak if fp_steps else peak
     fac = sv.factors()
 
     e2e = None
@@ -600,19 +605,25 @@ def main():
                        "parallelism": "p-range windows per rank" if world > 1 else "1 GPU"},
             "e2e": e2e,
             "gpu_launches": kernel_launches,
-            "roofline": {"bound": "int32-imad (64-bit Montgomery products)", "achieved": achieved, "peak": peak,
-                         "unit": "Gmulmod/s", "frac": achieved / peak,
+            "roofline": {"bound": ("fp64 pipe (FMA-based modular products, p < 2^51)" if fp_steps
+                                   else "int32-imad (64-bit Montgomery products)"),
+                         "achieved": achieved, "peak": rpeak, "unit": "Gmulmod/s", "frac": achieved / rpeak,
                          "traffic": BSGS_DRAM_BYTES_PER_PRIME * tot["primes"] / max(bsgs_launches, 1),
                          "traffic_unit": "bytes per BSGS launch (ncu per-prime DRAM bytes x primes per launch)",
                          "work_unit": "baby + giant steps of the BSGS kernel (each one modular product or "
                                       "doublings, plus one table insert or probe)",
-                         "peak_source": "measured live: rs_mulmod_peak, independent Montgomery-product chains",
+                         "peak_source": ("measured live: rs_fpmul_peak, independent chains of the steps' FP64 product"
+                                         if fp_steps else
+                                         "measured live: rs_mulmod_peak, independent Montgomery-product chains"),
+                         "peak_fp64_products": fpeak,
+                         "peak_montgomery_products": peak,
+                         "frac_of_montgomery_peak": achieved / peak,
                          "peak_multiplier": peak_mult,
                          "frac_of_multiplier_peak": achieved / peak_mult,
                          "peak_multiplier_source": "measured live: rs_widemul_peak (independent mad.wide.u32 "
                                                    "chains) / 11 wide products per Montgomery product",
                          "r_wide_per_sm_clock": (wide * 1e9 / (sms * clocks["sm_mhz"] * 1e6)) if clocks else None,
-                         "giant_only_frac": (tot["giant"] / max(bsgs_launches, 1)) / (bsgs_ms_avg / 1e3) / 1e9 / peak},
+                         "giant_only_frac": (tot["giant"] / max(bsgs_launches, 1)) / (bsgs_ms_avg / 1e3) / 1e9 / rpeak},
             "cpu_baseline": cpu,
             "forms": forms,
             "clocks": clocks,

@@ -272,6 +272,11 @@ int rs_mulmod_peak(rs_ctx *ctx, double *gmulmods_per_s, double *ms);
  * multiplier itself allows.  A measurement aid with no reference counterpart
  * (the reference reports no roofline). */
 int rs_widemul_peak(rs_ctx *ctx, double *gwide_per_s, double *ms);
+/* Throughput of independent FP64 modular products by a fixed multiplier (the
+ * product the BSGS steps use below 2^51: an exact two-product, a quotient from
+ * the double w/p, one correction), in 10^9 products/s, on a prime just above
+ * 2^50.  A measurement aid with no reference counterpart. */
+int rs_fpmul_peak(rs_ctx *ctx, double *gfpmul_per_s, double *ms);
 
 /* Largest range width (p1 - p0) that rs_primes_generate_noalloc accepts. */
 #define RS_NOALLOC_MAX_WIDTH (1ull << 22)

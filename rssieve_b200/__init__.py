@@ -50,7 +50,7 @@ EXPORTS = (
     "rs_factors_file_apply", "rs_factors_commit", "rs_factors_finalize", "rs_state_write", "rs_state_read",
     "rs_state_resume", "rs_ctx_create", "rs_ctx_destroy", "rs_ctx_set_stream", "rs_device_count",
     "rs_job_load", "rs_run_range", "rs_factors_fetch", "rs_bitmap_download", "rs_counters_get",
-    "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_widemul_peak", "rs_primes_generate_noalloc",
+    "rs_primes_generate", "rs_last_timing", "rs_mulmod_peak", "rs_widemul_peak", "rs_fpmul_peak", "rs_primes_generate_noalloc",
     "rs_set_baby_steps", "rs_get_baby_steps", "rs_set_wait_limit",
     "rs_batch_create", "rs_batch_destroy", "rs_batch_set_stream", "rs_batch_add", "rs_batch_add_clone",
     "rs_batch_free_slots", "rs_batch_job_bytes", "rs_batch_reserve", "rs_batch_release", "rs_batch_set_budget",
@@ -106,6 +106,7 @@ def lib():
                                      C.POINTER(u32)]),
         "rs_mulmod_peak": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "rs_widemul_peak": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "rs_fpmul_peak": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "rs_primes_generate_noalloc": (C.c_int, [u64, u64, vp, u32, vp, vp]),
         "rs_set_baby_steps": (C.c_int, [vp, u32]),
         "rs_batch_create": (C.c_int, [C.c_int, u32, u32, C.POINTER(vp)]),
@@ -360,6 +361,12 @@ class Sieve:
         """10^9 32x32->64 multiplies/s of independent chains on this device."""
         g, ms = C.c_double(0), C.c_double(0)
         _check(lib().rs_widemul_peak(self._c, C.byref(g), C.byref(ms)), "rs_widemul_peak")
+        return g.value
+
+    def fpmul_peak(self):
+        """10^9 FP64 modular products/s (the steps' product below 2^51) on this device."""
+        g, ms = C.c_double(0), C.c_double(0)
+        _check(lib().rs_fpmul_peak(self._c, C.byref(g), C.byref(ms)), "rs_fpmul_peak")
         return g.value
 
     def mulmod_peak(self):

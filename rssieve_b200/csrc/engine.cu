@@ -625,6 +625,28 @@ extern "C" int rs_widemul_peak(rs_ctx *c, double *gwide_per_s, double *ms_out)
     return RS_OK;
 }
 
+extern "C" int rs_fpmul_peak(rs_ctx *c, double *gfpmul_per_s, double *ms_out)
+{
+    if (!c || !gfpmul_per_s) return RS_EARG;
+    CU(cudaSetDevice(c->device));
+    const int blocks = c->sms * 8, iters = 4096;
+    u64 *out = nullptr;
+    CU(cudaMalloc(&out, (size_t)blocks * 256 * 8));
+    int rc = ensure_events(c, 2);
+    if (rc) { cudaFree(out); return rc; }
+    CU(launch_fpmul_peak(out, blocks, 64, c->stream));          // warm-up
+    CU(cudaEventRecord(c->ev[0], c->stream));
+    CU(launch_fpmul_peak(out, blocks, iters, c->stream));
+    CU(cudaEventRecord(c->ev[1], c->stream));
+    CU(cudaEventSynchronize(c->ev[1]));
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    cudaFree(out);
+    *gfpmul_per_s = (double)blocks * 256 * 8 * iters / (ms * 1e-3) / 1e9;
+    if (ms_out) *ms_out = ms;
+    return RS_OK;
+}
+
 extern "C" int rs_mulmod_peak(rs_ctx *c, double *gmulmods_per_s, double *ms_out)
 {
     if (!c || !gmulmods_per_s) return RS_EARG;

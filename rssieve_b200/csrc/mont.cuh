@@ -85,6 +85,19 @@ RS_DEV double fp_mulfix(double x, double w, double wq, double p)
     return (r < 0.0) ? r + p : r;
 }
 
+// x*y mod p on the FP64 pipe for two variable factors, p < 3*2^49, with pinv =
+// 1/p: as fp_mulfix, but the quotient rint(h*pinv) carries three roundings
+// (h, pinv, the product), a relative error below 3*2^-53, which stays below
+// 1/2 for t = x*y/p < p < 3*2^49; so again r lies in (-p, p).
+RS_DEV double fp_mul(double x, double y, double p, double pinv)
+{
+    const double h = x * y;
+    const double l = fma(x, y, -h);
+    const double q = rint(h * pinv);
+    const double r = fma(-q, p, h) + l;
+    return (r < 0.0) ? r + p : r;
+}
+
 // 2x mod p for x in [0, p), p < 2^52: exact in FP64.
 RS_DEV double fp_dbl(double x, double p)
 {

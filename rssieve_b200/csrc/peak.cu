@@ -3,8 +3,9 @@
 // independent dependency chains of the same mmul() the kernels use, so the
 // 32-bit IMAD pipe, not latency, is the limit, on a 62-bit prime) and the raw
 // 32x32->64 multiply throughput, from which the multiplier-bound product rate
-// is the wide-multiply rate / 11.  Rates are operations / kernel time (CUDA
-// events on the stream).
+// is the wide-multiply rate / 11, and the FP64 modular-product throughput of
+// the steps below 2^51.  Rates are operations / kernel time (CUDA events on
+// the stream).
 #include "mont.cuh"
 #include "rs_internal.h"
 
@@ -45,6 +46,33 @@ __global__ void __launch_bounds__(256) k_widemul_peak(u64 *out, u32 m, int iters
 #pragma unroll
     for (int j = 0; j < 16; ++j) x ^= c[j];
     out[t] = x;
+}
+
+// FP64 modular-product throughput: eight independent chains per thread of the
+// kernels' fp_mulfix by a fixed multiplier, on a prime just above 2^50 (the
+// 100-sequence benchmark's p-range), where the BSGS steps use it.
+__global__ void __launch_bounds__(256) k_fpmul_peak(u64 *out, double p, double w, double wq, int iters)
+{
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    double a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = (double)(t * 8ull + j + 1);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = fp_mulfix(a[j], w, wq, p);
+    }
+    u64 x = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x ^= (u64)a[j];
+    out[t] = x;
+}
+
+cudaError_t launch_fpmul_peak(u64 *out, int blocks, int iters, cudaStream_t st)
+{
+    const u64 p = 1125899906842679ull;       // prime just above 2^50
+    const u64 w = 0x123456789ABCull % p;
+    k_fpmul_peak<<<blocks, 256, 0, st>>>(out, (double)p, (double)w, (double)w / (double)p, iters);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_widemul_peak(u64 *out, int blocks, int iters, cudaStream_t st)

@@ -114,6 +114,9 @@ struct JobDev {
 // mont.cuh): residues are exact integers in doubles, and a product by a fixed
 // multiplier w takes its quotient from the double w/p.
 constexpr u64 FP_BOUND = 1ull << 51;
+// Below FP_MUL_BOUND = 3*2^49 the set-up's chi chains (products of two
+// variable factors, fp_mul) run on the FP64 pipe as well.
+constexpr u64 FP_MUL_BOUND = 3ull << 49;
 
 struct PrimeHdr {        // 128 bytes (a 16-byte multiple: copied by TMA bulk copies)
     u64 p;               // 0 = skipped
@@ -218,6 +221,7 @@ size_t bsgs_smem_bytes(int geom);
 cudaError_t bsgs_prepare();   // per device, before the first launch
 cudaError_t launch_mulmod_peak(u64 *out, int blocks, int iters, cudaStream_t st);
 cudaError_t launch_widemul_peak(u64 *out, int blocks, int iters, cudaStream_t st);
+cudaError_t launch_fpmul_peak(u64 *out, int blocks, int iters, cudaStream_t st);
 
 // batch rounds (sieve.cu, setup.cu, bsgs.cu)
 // win[r]: primes range slot r should cover this round (0: none); capped at 0.6*rcap

@@ -245,6 +245,41 @@ __device__ __forceinline__ void mpow_lanes(u32 R, u64 (&a)[4], const u64 (&x)[4]
     else mpow_multi<4, LAZY>(a, x, ex, M);
 }
 
+// The chains of mpow_multi on the FP64 pipe (p < FP_MUL_BOUND): plain residues
+// held exactly in doubles, products by fp_mul.
+template <int R>
+__device__ __forceinline__ void fpow_multi(double (&a)[4], const double (&x)[4], u64 ex, double pd, double pinv)
+{
+#pragma unroll
+    for (int r = 0; r < R; ++r) a[r] = x[r];
+    for (int bit = 62 - __clzll(ex); bit >= 0; --bit) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r] = fp_mul(a[r], a[r], pd, pinv);
+        if ((ex >> bit) & 1) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) a[r] = fp_mul(a[r], x[r], pd, pinv);
+        }
+    }
+}
+
+// At most two chains at a time: FP64 products have short enough latencies,
+// and four interleaved chains would not fit the kernel's 64 registers.
+__device__ __forceinline__ void fpow_lanes(u32 R, double (&a)[4], const double (&x)[4], u64 ex, double pd, double pinv)
+{
+    if (R == 1) {
+        fpow_multi<1>(a, x, ex, pd, pinv);
+        return;
+    }
+    fpow_multi<2>(a, x, ex, pd, pinv);
+    if (R > 2) {
+        double a2[4], x2[4] = {x[2], x[3], x[3], x[3]};
+        if (R == 3) fpow_multi<1>(a2, x2, ex, pd, pinv);
+        else fpow_multi<2>(a2, x2, ex, pd, pinv);
+        a[2] = a2[0];
+        a[3] = a2[1];
+    }
+}
+
 // Sequence classes, targets, baby-step count and the start tables of record w
 // (one warp).  tw: this warp's two tables of SPLIT_MAX entries in shared memory.
 __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 w, u32 lane, PrimeHdr *__restrict__ hdr,
@@ -278,7 +313,19 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     // exponent for the whole warp, R independent chains per lane
     const u32 R = (K + 31) / 32;
     u64 z[4];
-    {
+    if (p < FP_MUL_BOUND) {
+        double x[4], zd[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const u32 i = lane + 32 * r;
+            const u64 kv = (i < K) ? job->k[i] : 1;
+            x[r] = (double)((kv < p) ? kv : kv % p);
+        }
+        const double pd = (double)p;
+        fpow_lanes(R, zd, x, X.xD, pd, 1.0 / pd);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) z[r] = to_mont((u64)zd[r], M);
+    } else {
         u64 x[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {

@@ -120,6 +120,19 @@ def test_config2_job_planted_across_2_51_and_at_2_62(sieve, oracle, rs):
     assert all((s, n) in got for s, n, _ in planted)
 
 
+def test_config2_job_planted_across_3_2_49(sieve, oracle, rs):
+    """Planted factors on both sides of 3*2^49, where the set-up's chi chains
+    change from FP64 products (largest quotient error just below it) to lazy
+    Montgomery products."""
+    mid = 3 << 49
+    job, lo = plant_job(oracle, W.config2(2), mid - 8192, mid, 6, 1 << 32, 1, seqs=list(range(1, 100, 8)))
+    job, hi = plant_job(oracle, job, mid, mid + 8192, 6, 1 << 32, 1, seqs=list(range(5, 100, 8)))
+    assert len(lo) >= 4 and len(hi) >= 4
+    fac = _check_single(sieve, oracle, rs, job, mid - 8192, mid + 8192, len(lo) + len(hi))
+    got = _terms(fac)
+    assert all((s, n) in got for s, n, _ in lo + hi)
+
+
 def test_config4_job_planted_near_2_64(sieve, oracle, rs):
     """The config-4 job (b = 5, 20 sequences, k even < 2^40, c alternating) with
     sequences re-drawn so that primes of the first 2^16 of its p-range, just
