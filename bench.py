@@ -35,11 +35,11 @@ WORKLOAD = ("config2 plain form: 100 seqs k*2^n+-1 (50 +1, 50 -1), k odd U[3,2^3
             "kept w.p. 0.03, p windows from 2^50")
 P_START = 1 << 50
 # DRAM bytes (read + write) per prime of the BSGS kernel, from one ncu capture
-# of a 2^20-wide window at 2^50 at the tuned Q = 8192 (64.42 MB for 30 203
-# primes): the 2112-byte prime record plus claims.  Traffic grows in proportion
-# to primes, so the per-launch figure is this times the primes one launch
-# processes.
-BSGS_DRAM_BYTES_PER_PRIME = 2132.9
+# of a 2^20-wide window at 2^50 at the tuned Q = 8192 (69.18 MB for 30 203
+# primes, FP64 steps): the 2272-byte prime record plus claims.  Traffic grows
+# in proportion to primes, so the per-launch figure is this times the primes
+# one launch processes.
+BSGS_DRAM_BYTES_PER_PRIME = 2290.5
 
 
 def reference_params(nmin, nmax):

@@ -67,7 +67,7 @@ struct BJob {
     std::vector<u32> ranges;
 };
 
-constexpr int NGROUP = 2 * NGEOM;  // BSGS groups: g = 2*geometry + (1 for Shoup products below 2^63)
+constexpr int NGROUP = 3 * NGEOM;  // BSGS groups: g = 3*geometry + step kind (2 FP64, 1 Shoup, 0 Montgomery)
 
 __global__ void k_batch_account(const BatchRange *ranges, const u32 *ctrs, u32 rcap, u32 nranges, u64 *range_primes,
                                 u64 *stats, u32 *unfinished)
@@ -118,6 +118,7 @@ struct rs_batch {
     u64 *d_mid = nullptr;                  // base-2 probable primes of all ranges awaiting the Lucas pass
     u32 *d_mid_r = nullptr;                //   and their ranges (R * CCAP entries)
     u32 *d_mid_ctr = nullptr;
+    u32 *d_rec_of = nullptr;               // record index of each prime of a round (R * RCAP)
     PrimeHdr *d_hdr = nullptr;
     void *d_aux = nullptr;
     u64 *d_tabs = nullptr, *d_tgt = nullptr;
@@ -163,7 +164,7 @@ extern "C" void rs_batch_destroy(rs_batch *b)
     void *ptrs[] = {b->d_sp, b->d_jobs, b->d_geoms, b->d_args, b->d_fctrs, b->d_ranges, b->d_wins, b->d_ctrs,
                     b->d_range_primes, b->d_cands, b->d_primes, b->d_hdr, b->d_aux, b->d_tabs, b->d_tgt, b->d_meta,
                     b->d_err, b->d_stats, b->d_unfinished, b->d_win, b->d_prefix_c, b->d_prefix_p,
-                    b->d_gprefix, b->d_gwork, b->d_mid, b->d_mid_r, b->d_mid_ctr};
+                    b->d_gprefix, b->d_gwork, b->d_mid, b->d_mid_r, b->d_mid_ctr, b->d_rec_of};
     for (void *p : ptrs) cudaFree(p);
     if (b->h_pin) cudaFreeHost(b->h_pin);
     if (b->h_win_pin) cudaFreeHost(b->h_win_pin);
@@ -216,7 +217,7 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         !alloc((void **)&b->d_ctrs, (size_t)R * BR_CTRS * 4) || !alloc((void **)&b->d_range_primes, R * 8) ||
         !alloc((void **)&b->d_cands, (size_t)R * CCAP * 8) || !alloc((void **)&b->d_primes, (size_t)R * RCAP * 8) ||
         !alloc((void **)&b->d_mid, (size_t)R * CCAP * 8) || !alloc((void **)&b->d_mid_r, (size_t)R * CCAP * 4) ||
-        !alloc((void **)&b->d_mid_ctr, 4) ||
+        !alloc((void **)&b->d_mid_ctr, 4) || !alloc((void **)&b->d_rec_of, (size_t)R * RCAP * 4) ||
         !alloc((void **)&b->d_hdr, (size_t)R * RCAP * sizeof(PrimeHdr)) ||
         !alloc(&b->d_aux, (size_t)R * RCAP * setup_aux_bytes()) ||
         !alloc((void **)&b->d_tabs, (size_t)R * RCAP * TABS * 8) ||
@@ -225,7 +226,7 @@ extern "C" int rs_batch_create(int device, uint32_t max_jobs, uint32_t range_slo
         !alloc((void **)&b->d_prefix_c, (R + 1) * 4) || !alloc((void **)&b->d_prefix_p, (R + 1) * 4) ||
         cudaMallocHost(&b->h_pin, 16) != cudaSuccess || cudaMallocHost(&b->h_win_pin, R * 4) != cudaSuccess) {
         rs_set_error("cannot allocate a batch of %u range slots (about %zu MB)", R,
-                     (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 10 + 24 + 8 + 16 + 24) >> 20);
+                     (size_t)R * RCAP * (sizeof(PrimeHdr) + TABS * 8 + KSTRIDE * 10 + 24 + 8 + 16 + 24 + 4) >> 20);
         return fail(RS_ENOMEM);
     }
     if (cudaMemcpy(b->d_sp, sp.data(), sp.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -299,7 +300,8 @@ extern "C" int rs_batch_add(rs_batch *b, const rs_seqs *s, uint64_t p0, uint64_t
 
 // Adds a job from host sequences s, or (s == nullptr) as a copy of job slot src
 // made on the device.  p0 == p1: a resident template that takes no range slot.
-// The p-range is cut into nsplit equal parts, and at 2^63, one range slot each.
+// The p-range is cut into nsplit equal parts, and at 2^51 and 2^63 (where the
+// BSGS step kind changes), one range slot each.
 static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_t p0, uint64_t p1, uint32_t q,
                          uint32_t nsplit, uint32_t *job)
 {
@@ -318,6 +320,7 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
         cuts.push_back(p0);
         for (u32 i = 1; i < nsplit; ++i) cuts.push_back(p0 + i * w);
         if (p0 < TOP && p1 > TOP) cuts.push_back(TOP);
+        if (p0 < FP_BOUND && p1 > FP_BOUND) cuts.push_back(FP_BOUND);
         cuts.push_back(p1);
         std::sort(cuts.begin(), cuts.end());
         cuts.erase(std::unique(cuts.begin(), cuts.end()), cuts.end());
@@ -392,7 +395,7 @@ static int batch_add_job(rs_batch *b, const rs_seqs *s, const BJob *src, uint64_
         R.p_end = hi;
         R.job = jid;
         R.active = 1;
-        R.shoup = (hi <= TOP) ? 1 : 0;
+        R.mode = (hi <= FP_BOUND) ? 2 : (hi <= TOP) ? 1 : 0;
         R.geom = (u8)J.geom;
         b->h_ranges[r] = R;
         b->range_used[r] = 1;
@@ -491,7 +494,8 @@ static int batch_round(rs_batch *b)
                          R * CCAP, b->d_mid_ctr, b->d_err, b->sms, st));
     BCU(launch_batch_prefix_all(b->d_ranges, R, 1, RCAP, b->d_ctrs, b->d_prefix_p, st));
     BCU(launch_setup_batch(b->d_jobs, b->d_geoms, b->d_ranges, b->d_primes, RCAP, b->d_prefix_p, R, b->d_hdr,
-                           b->d_aux, b->d_tabs, b->d_tgt, b->d_meta, b->d_stats, b->d_err, b->sms, st));
+                           b->d_aux, b->d_tabs, b->d_tgt, b->d_meta, b->d_stats, b->d_err, b->d_rec_of, b->sms,
+                           st));
     BsgsArgs a;
     memset(&a, 0, sizeof a);
     a.stats = b->d_stats;
@@ -504,7 +508,7 @@ static int batch_round(rs_batch *b)
     for (int g = 0; g < NGROUP; ++g) {
         BCU(cudaStreamWaitEvent(b->side[g], b->fork, 0));
         BCU(launch_bsgs_batch(a, b->d_args, b->d_hdr, b->d_tabs, b->d_tgt, b->d_meta, R,
-                              b->d_gprefix + (size_t)g * (R + 1), RCAP, b->d_gwork + g, (g & 1) != 0, g >> 1, b->sms,
+                              b->d_gprefix + (size_t)g * (R + 1), RCAP, b->d_gwork + g, g % 3, g / 3, b->sms,
                               b->side[g]));
         BCU(cudaEventRecord(b->join[g], b->side[g]));
         BCU(cudaStreamWaitEvent(st, b->join[g], 0));

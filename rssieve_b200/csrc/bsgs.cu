@@ -764,7 +764,7 @@ cudaError_t launch_bsgs(const BsgsArgs &a, const PrimeHdr *hdr, const u64 *tabs,
 // (capped at rcap) when it is active and in the (geom, shoup) group -- or, for
 // geom < 0, when it is active -- else + 0.  One block of 256 threads: each
 // sums a contiguous run of slots, a block scan offsets the runs.
-__global__ void __launch_bounds__(256) k_batch_prefix(const BatchRange *ranges, u32 nr, int geom, int shoup,
+__global__ void __launch_bounds__(256) k_batch_prefix(const BatchRange *ranges, u32 nr, int geom, int mode,
                                                       const u32 *ctrs, u32 rcap, u32 *prefix, int which)
 {
     __shared__ u32 part[256];
@@ -773,7 +773,7 @@ __global__ void __launch_bounds__(256) k_batch_prefix(const BatchRange *ranges, 
     const u32 k0 = t * per, k1 = min(k0 + per, nr);
     auto cnt = [&](u32 k) -> u32 {
         const BatchRange R = ranges[k];
-        const bool in = R.active && (geom < 0 || (R.geom == geom && R.shoup == shoup));
+        const bool in = R.active && (geom < 0 || (R.geom == geom && R.mode == mode));
         return in ? min(ctrs[k * BR_CTRS + which], rcap) : 0u;
     };
     u32 sum = 0;
@@ -795,14 +795,14 @@ __global__ void __launch_bounds__(256) k_batch_prefix(const BatchRange *ranges, 
 }
 
 // Every BSGS group's prefix sums in one launch: block g computes those of
-// group g = 2*geometry + (1 for Shoup products) into prefix + g*(nr+1) and
+// group g = 3*geometry + step kind (BatchRange::mode) into prefix + g*(nr+1) and
 // clears the group's work counter.
 __global__ void __launch_bounds__(256) k_batch_group_prefix(const BatchRange *ranges, u32 nr, const u32 *ctrs,
                                                             u32 rcap, u32 *prefix, u32 *work)
 {
     __shared__ u32 part[256];
     const u32 g = blockIdx.x;
-    const int geom = (int)(g >> 1), shoup = (int)(g & 1);
+    const int geom = (int)(g / 3), mode = (int)(g % 3);
     u32 *pf = prefix + (size_t)g * (nr + 1);
     const u32 t = threadIdx.x;
     if (t == 0) work[g] = 0;
@@ -810,7 +810,7 @@ __global__ void __launch_bounds__(256) k_batch_group_prefix(const BatchRange *ra
     const u32 k0 = t * per, k1 = min(k0 + per, nr);
     auto cnt = [&](u32 k) -> u32 {
         const BatchRange R = ranges[k];
-        const bool in = R.active && R.geom == geom && R.shoup == shoup;
+        const bool in = R.active && R.geom == geom && R.mode == mode;
         return in ? min(ctrs[k * BR_CTRS + 1], rcap) : 0u;
     };
     u32 sum = 0;
@@ -834,7 +834,7 @@ __global__ void __launch_bounds__(256) k_batch_group_prefix(const BatchRange *ra
 cudaError_t launch_batch_group_prefix(const BatchRange *ranges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix,
                                       u32 *work, cudaStream_t st)
 {
-    k_batch_group_prefix<<<2 * NGEOM, 256, 0, st>>>(ranges, nr, ctrs, rcap, prefix, work);
+    k_batch_group_prefix<<<3 * NGEOM, 256, 0, st>>>(ranges, nr, ctrs, rcap, prefix, work);
     return cudaGetLastError();
 }
 
@@ -847,14 +847,16 @@ cudaError_t launch_batch_prefix_all(const BatchRange *ranges, u32 nr, int which,
 
 cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
                               const u64 *tgt, const unsigned short *meta, u32 nr, const u32 *prefix, u32 rcap,
-                              u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st)
+                              u32 *work_ctr, int mode, int geom, int sms, cudaStream_t st)
 {
-#define RS_BSGS_BCASE(G)                                                                                         \
-    case G:                                                                                                      \
-        return shoup ? launch_geom<G, 1, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, nr, prefix, \
-                                               rcap)                                                             \
-                     : launch_geom<G, 0, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, nr, prefix, \
-                                               rcap);
+#define RS_BSGS_BCASE(G)                                                                                           \
+    case G:                                                                                                        \
+        return mode == 2 ? launch_geom<G, 2, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, nr, prefix, \
+                                                   rcap)                                                           \
+             : mode == 1 ? launch_geom<G, 1, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, nr, prefix, \
+                                                   rcap)                                                           \
+                         : launch_geom<G, 0, true>(a, hdr, tabs, tgt, meta, 0, work_ctr, sms, st, job_args, nr, prefix, \
+                                                   rcap);
     switch (geom) {
         RS_BSGS_BCASE(0)
         RS_BSGS_BCASE(1)

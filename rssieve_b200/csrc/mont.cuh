@@ -85,15 +85,19 @@ RS_DEV double fp_mulfix(double x, double w, double wq, double p)
     return (r < 0.0) ? r + p : r;
 }
 
-// x*y mod p on the FP64 pipe for two variable factors, p < 3*2^49, with pinv =
-// 1/p: as fp_mulfix, but the quotient rint(h*pinv) carries three roundings
-// (h, pinv, the product), a relative error below 3*2^-53, which stays below
-// 1/2 for t = x*y/p < p < 3*2^49; so again r lies in (-p, p).
+// x*y mod p on the FP64 pipe for two variable factors, with pinv = 1/p: as
+// fp_mulfix, but the quotient comes from pinv.  rint(h*pinv) carries three
+// roundings (h, pinv, the product), a relative error below 3*2^-53, which
+// stays below 1/2 for t = x*y/p < p < 3*2^49.  WIDE (p < 2^51) forms the
+// quotient as fma(h, pinv, l*pinv), i.e. from the exact h + l: two roundings
+// that matter (pinv, the fma; l*pinv is below 2^-2 in magnitude), a relative
+// error below 2^-52, below 1/2 for t < 2^51.  Either way r lies in (-p, p).
+template <bool WIDE = false>
 RS_DEV double fp_mul(double x, double y, double p, double pinv)
 {
     const double h = x * y;
     const double l = fma(x, y, -h);
-    const double q = rint(h * pinv);
+    const double q = rint(WIDE ? fma(h, pinv, l * pinv) : h * pinv);
     const double r = fma(-q, p, h) + l;
     return (r < 0.0) ? r + p : r;
 }

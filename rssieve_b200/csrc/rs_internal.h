@@ -114,8 +114,9 @@ struct JobDev {
 // mont.cuh): residues are exact integers in doubles, and a product by a fixed
 // multiplier w takes its quotient from the double w/p.
 constexpr u64 FP_BOUND = 1ull << 51;
-// Below FP_MUL_BOUND = 3*2^49 the set-up's chi chains (products of two
-// variable factors, fp_mul) run on the FP64 pipe as well.
+// The set-up's chi chains (products of two variable factors, fp_mul) run on
+// the FP64 pipe below FP_BOUND as well, with a shorter quotient below
+// FP_MUL_BOUND = 3*2^49.
 constexpr u64 FP_MUL_BOUND = 3ull << 49;
 
 struct PrimeHdr {        // 128 bytes (a 16-byte multiple: copied by TMA bulk copies)
@@ -169,7 +170,7 @@ struct BatchRange {      // device state of one range slot
     u64 p_cur, p_end;    // next window start, end of the range
     u32 job;             // job slot it belongs to
     u8 active;           // slot in use
-    u8 shoup;            // 1: p_end <= 2^63 (Shoup giant steps), 0: p >= 2^63
+    u8 mode;             // BSGS step kind: 2 p_end <= 2^51 (FP64), 1 p_end <= 2^63 (Shoup), 0 p >= 2^63
     u8 geom;             // BSGS geometry index of its job
     u8 pad_;
 };
@@ -236,11 +237,13 @@ cudaError_t launch_sieve_batch(const BatchWin *wins, u32 nranges, u32 max_blocks
 cudaError_t launch_mr_batch2(const u64 *cands, u32 ccap, u64 *primes, u32 rcap, u32 *ctrs, u32 nranges,
                              const u32 *prefix_c, u64 *mid, u32 *mid_r, u32 mid_cap, u32 *mid_ctr, u32 *err, int sms,
                              cudaStream_t st);
-// set-up of the primes of all ranges (prefix_p: prefix sums of their counts)
+// set-up of the primes of all ranges (prefix_p: prefix sums of their counts;
+// rec_of: room for one record index per prime, nranges * rcap)
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
                                u32 rcap, const u32 *prefix_p, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs,
-                               u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, int sms, cudaStream_t st);
-// one BSGS launch per (geometry, mode) group g = 2*geometry + shoup over range
+                               u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, u32 *rec_of, int sms,
+                               cudaStream_t st);
+// one BSGS launch per (geometry, mode) group g = 3*geometry + mode over range
 // slots [0, nr): prefix + g*(nr+1) (nr+1 entries) counts the primes of the
 // active slots of that group only; work[g] is cleared
 cudaError_t launch_batch_group_prefix(const BatchRange *ranges, u32 nr, const u32 *ctrs, u32 rcap, u32 *prefix,
@@ -250,7 +253,7 @@ cudaError_t launch_batch_prefix_all(const BatchRange *ranges, u32 nr, int which,
                                     u32 *prefix, cudaStream_t st);
 cudaError_t launch_bsgs_batch(const BsgsArgs &a, const BsgsArgs *job_args, const PrimeHdr *hdr, const u64 *tabs,
                               const u64 *tgt, const unsigned short *meta, u32 nr, const u32 *prefix, u32 rcap,
-                              u32 *work_ctr, bool shoup, int geom, int sms, cudaStream_t st);
+                              u32 *work_ctr, int mode, int geom, int sms, cudaStream_t st);
 
 }  // namespace rs
 

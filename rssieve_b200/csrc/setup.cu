@@ -165,14 +165,16 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
 // Kernel 1.  Single job: primes[first, first+count) into records [0, count).
 // Batch (BATCH): the primes of every range as one index space (prefix: prefix
 // sums of the ranges' prime counts); prime i of range r is record r*rcap + i,
-// with its job's sequences.
+// with its job's sequences.  rec_of[i] keeps that record index, so kernels 2
+// and 3 need no search over the prefix sums.
 template <bool BATCH>
 __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ jobs, const u64 *__restrict__ primes,
                                                      u32 first, u32 count, PrimeHdr *__restrict__ hdr,
                                                      PrimeAux *__restrict__ aux, JobGeom gm,
                                                      const JobGeom *__restrict__ geoms,
                                                      const BatchRange *__restrict__ ranges,
-                                                     const u32 *__restrict__ prefix, u32 nr, u32 rcap)
+                                                     const u32 *__restrict__ prefix, u32 nr, u32 rcap,
+                                                     u32 *__restrict__ rec_of)
 {
     const u32 stride = gridDim.x * blockDim.x;
     if constexpr (BATCH) {
@@ -181,6 +183,7 @@ __global__ void __launch_bounds__(256) k_setup_prime(const JobDev *__restrict__ 
             const u32 r = prefix_find(prefix, nr, i);
             const u32 rec = r * rcap + (i - prefix[r]);
             const u32 jb = ranges[r].job;
+            rec_of[i] = rec;
             setup_prime_one(jobs + jb, primes[rec], rec, jb, hdr, aux, geoms[jb]);
         }
     } else {
@@ -245,39 +248,79 @@ __device__ __forceinline__ void mpow_lanes(u32 R, u64 (&a)[4], const u64 (&x)[4]
     else mpow_multi<4, LAZY>(a, x, ex, M);
 }
 
-// The chains of mpow_multi on the FP64 pipe (p < FP_MUL_BOUND): plain residues
-// held exactly in doubles, products by fp_mul.
-template <int R>
+// The chains of mpow_multi on the FP64 pipe (p < FP_BOUND): plain residues
+// held exactly in doubles, products by fp_mul (its WIDE quotient from
+// FP_MUL_BOUND on).
+template <int R, bool WIDE>
 __device__ __forceinline__ void fpow_multi(double (&a)[4], const double (&x)[4], u64 ex, double pd, double pinv)
 {
 #pragma unroll
     for (int r = 0; r < R; ++r) a[r] = x[r];
     for (int bit = 62 - __clzll(ex); bit >= 0; --bit) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[r] = fp_mul(a[r], a[r], pd, pinv);
+        for (int r = 0; r < R; ++r) a[r] = fp_mul<WIDE>(a[r], a[r], pd, pinv);
         if ((ex >> bit) & 1) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) a[r] = fp_mul(a[r], x[r], pd, pinv);
+            for (int r = 0; r < R; ++r) a[r] = fp_mul<WIDE>(a[r], x[r], pd, pinv);
         }
     }
 }
 
 // At most two chains at a time: FP64 products have short enough latencies,
 // and four interleaved chains would not fit the kernel's 64 registers.
+template <bool WIDE>
 __device__ __forceinline__ void fpow_lanes(u32 R, double (&a)[4], const double (&x)[4], u64 ex, double pd, double pinv)
 {
     if (R == 1) {
-        fpow_multi<1>(a, x, ex, pd, pinv);
+        fpow_multi<1, WIDE>(a, x, ex, pd, pinv);
         return;
     }
-    fpow_multi<2>(a, x, ex, pd, pinv);
+    fpow_multi<2, WIDE>(a, x, ex, pd, pinv);
     if (R > 2) {
         double a2[4], x2[4] = {x[2], x[3], x[3], x[3]};
-        if (R == 3) fpow_multi<1>(a2, x2, ex, pd, pinv);
-        else fpow_multi<2>(a2, x2, ex, pd, pinv);
+        if (R == 3) fpow_multi<1, WIDE>(a2, x2, ex, pd, pinv);
+        else fpow_multi<2, WIDE>(a2, x2, ex, pd, pinv);
         a[2] = a2[0];
         a[3] = a2[1];
     }
+}
+
+// z[r] = chi(k_i) = k_i^xD in Montgomery form for the lane's sequences
+// i = lane + 32r < K (1 elsewhere).  (Out of line, with the caller's state
+// saved once per prime instead of spilled, it measured 3-6% slower.)
+struct Chi4 {
+    u64 z[4];
+};
+__device__ __forceinline__ Chi4 chi_of_ks(const JobDev *__restrict__ job, u32 lane, u32 K, const Mont M, u64 xD)
+{
+    const u64 p = M.p;
+    const u32 R = (K + 31) / 32;
+    Chi4 out;
+    if (p < FP_BOUND) {
+        double x[4], zd[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const u32 i = lane + 32 * r;
+            const u64 kv = (i < K) ? job->k[i] : 1;
+            x[r] = (double)((kv < p) ? kv : kv % p);
+        }
+        const double pd = (double)p;
+        if (p < FP_MUL_BOUND) fpow_lanes<false>(R, zd, x, xD, pd, 1.0 / pd);
+        else fpow_lanes<true>(R, zd, x, xD, pd, 1.0 / pd);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) out.z[r] = to_mont((u64)zd[r], M);
+    } else {
+        u64 x[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const u32 i = lane + 32 * r;
+            const u64 kv = (i < K) ? job->k[i] : 1;
+            x[r] = to_mont((kv < p) ? kv : kv % p, M);
+        }
+        if (p >> 62) mpow_lanes<false>(R, out.z, x, xD, M);
+        else mpow_lanes<true>(R, out.z, x, xD, M);
+    }
+    return out;
 }
 
 // Sequence classes, targets, baby-step count and the start tables of record w
@@ -312,30 +355,8 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     // z = chi(k) = k^xD for the lane's sequences i = lane + 32r, r < R: one
     // exponent for the whole warp, R independent chains per lane
     const u32 R = (K + 31) / 32;
-    u64 z[4];
-    if (p < FP_MUL_BOUND) {
-        double x[4], zd[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const u32 i = lane + 32 * r;
-            const u64 kv = (i < K) ? job->k[i] : 1;
-            x[r] = (double)((kv < p) ? kv : kv % p);
-        }
-        const double pd = (double)p;
-        fpow_lanes(R, zd, x, X.xD, pd, 1.0 / pd);
-#pragma unroll
-        for (int r = 0; r < 4; ++r) z[r] = to_mont((u64)zd[r], M);
-    } else {
-        u64 x[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const u32 i = lane + 32 * r;
-            const u64 kv = (i < K) ? job->k[i] : 1;
-            x[r] = to_mont((kv < p) ? kv : kv % p, M);
-        }
-        if (p >> 62) mpow_lanes<false>(R, z, x, X.xD, M);
-        else mpow_lanes<true>(R, z, x, X.xD, M);
-    }
+    const Chi4 zc = chi_of_ks(job, lane, K, M, X.xD);
+    const u64 (&z)[4] = zc.z;
     __syncwarp();
     // pass 1: the class of every sequence; the kept ones' k mod p and class
     // offset go to the record (compacted), the target itself once Q' is known
@@ -491,17 +512,16 @@ __global__ void __launch_bounds__(256) k_setup_tabs(const JobDev *__restrict__ j
                                                     const PrimeAux *__restrict__ aux, u32 count,
                                                     u64 *__restrict__ tabs, u64 *__restrict__ stats, JobGeom gm,
                                                     const JobGeom *__restrict__ geoms,
-                                                    const BatchRange *__restrict__ ranges,
-                                                    const u32 *__restrict__ prefix, u32 nr, u32 rcap)
+                                                    const u32 *__restrict__ prefix, u32 nr,
+                                                    const u32 *__restrict__ rec_of)
 {
     const u32 stride = gridDim.x * blockDim.x;
     u32 nt = 0, nf = 0, ns = 0;
     if constexpr (BATCH) {
         const u32 total = prefix[nr];
         for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-            const u32 r = prefix_find(prefix, nr, i);
-            const u32 rec = r * rcap + (i - prefix[r]);
-            const u32 jb = ranges[r].job;
+            const u32 rec = rec_of[i];
+            const u32 jb = hdr[rec].job;
             setup_tabs_one(jobs + jb, rec, hdr, aux, tabs, geoms[jb], nt, nf, ns);
         }
     } else {
@@ -528,8 +548,8 @@ __global__ void __launch_bounds__(SETUP_TPB, 4) k_setup_k(const JobDev *__restri
                                                        unsigned short *__restrict__ meta, u64 *__restrict__ stats,
                                                        u32 *__restrict__ err, JobGeom gm,
                                                        const JobGeom *__restrict__ geoms,
-                                                       const BatchRange *__restrict__ ranges,
-                                                       const u32 *__restrict__ prefix, u32 nr, u32 rcap)
+                                                       const u32 *__restrict__ prefix, u32 nr,
+                                                       const u32 *__restrict__ rec_of)
 {
     __shared__ u64 s_tw[SETUP_TPB / 32][2 * SPLIT_MAX];   // per warp: class and target tables of its prime
     const u32 lane = threadIdx.x & 31;
@@ -539,9 +559,8 @@ __global__ void __launch_bounds__(SETUP_TPB, 4) k_setup_k(const JobDev *__restri
     if constexpr (BATCH) {
         const u32 total = prefix[nr];
         for (u32 i = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5; i < total; i += nwarps) {
-            const u32 r = prefix_find(prefix, nr, i);
-            const u32 rec = r * rcap + (i - prefix[r]);
-            const u32 jb = ranges[r].job;
+            const u32 rec = rec_of[i];
+            const u32 jb = hdr[rec].job;
             setup_k_one(jobs + jb, rec, lane, hdr, aux, tabs, tgt, meta, stats, err, geoms[jb], tw);
         }
     } else {
@@ -556,36 +575,36 @@ cudaError_t launch_setup(const JobDev *job, const u64 *primes, u32 first, u32 co
     if (count == 0) return cudaSuccess;
     const JobGeom gm = job_geom(geom);
     k_setup_prime<false><<<(count + 255) / 256, 256, 0, st>>>(job, primes, first, count, hdr, (PrimeAux *)aux, gm,
-                                                              nullptr, nullptr, nullptr, 0, 0);
+                                                              nullptr, nullptr, nullptr, 0, 0, nullptr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const u32 wpb = SETUP_TPB / 32;
     k_setup_k<false><<<(count + wpb - 1) / wpb, SETUP_TPB, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, tgt,
-                                                                   meta, stats, err, gm, nullptr, nullptr, nullptr, 0,
-                                                                   0);
+                                                                   meta, stats, err, gm, nullptr, nullptr, 0, nullptr);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_setup_tabs<false><<<(count + 255) / 256, 256, 0, st>>>(job, hdr, (const PrimeAux *)aux, count, tabs, stats, gm,
-                                                             nullptr, nullptr, nullptr, 0, 0);
+                                                             nullptr, nullptr, 0, nullptr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_setup_batch(const JobDev *jobs, const JobGeom *geoms, const BatchRange *ranges, const u64 *primes,
                                u32 rcap, const u32 *prefix_p, u32 nranges, PrimeHdr *hdr, void *aux, u64 *tabs,
-                               u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, int sms, cudaStream_t st)
+                               u64 *tgt, unsigned short *meta, u64 *stats, u32 *err, u32 *rec_of, int sms,
+                               cudaStream_t st)
 {
     JobGeom gm{};
     // full-device grids; the kernels stride over the primes of every range
     k_setup_prime<true><<<sms * 4, 256, 0, st>>>(jobs, primes, 0, 0, hdr, (PrimeAux *)aux, gm, geoms, ranges,
-                                                 prefix_p, nranges, rcap);
+                                                 prefix_p, nranges, rcap, rec_of);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_setup_k<true><<<sms * 4, SETUP_TPB, 0, st>>>(jobs, hdr, (const PrimeAux *)aux, 0, tabs, tgt, meta, stats, err,
-                                                   gm, geoms, ranges, prefix_p, nranges, rcap);
+                                                   gm, geoms, prefix_p, nranges, rec_of);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_setup_tabs<true><<<sms * 4, 256, 0, st>>>(jobs, hdr, (const PrimeAux *)aux, 0, tabs, stats, gm, geoms, ranges,
-                                                prefix_p, nranges, rcap);
+    k_setup_tabs<true><<<sms * 4, 256, 0, st>>>(jobs, hdr, (const PrimeAux *)aux, 0, tabs, stats, gm, geoms,
+                                                prefix_p, nranges, rec_of);
     return cudaGetLastError();
 }
 

@@ -102,9 +102,10 @@ def test_config2_job_planted_at_2_50(sieve, oracle, rs):
 
 def test_config2_job_planted_across_2_51_and_at_2_62(sieve, oracle, rs):
     """The config-2 job with sequences re-drawn so that primes on both sides of
-    2^51 (the engine splits the window there: FP64 baby and giant steps below,
-    Shoup steps above) and primes of a window at 2^62 (Shoup steps; k < 2^40
-    there, so that small enough k exist) divide candidate terms."""
+    2^51 (the engine splits the window there: FP64 baby and giant steps and chi
+    chains below, Shoup steps and lazy Montgomery chains above) and primes of
+    a window at 2^62 (Shoup steps; k < 2^40 there, so that small enough k
+    exist) divide candidate terms."""
     mid = 1 << 51
     job, lo = plant_job(oracle, W.config2(2), mid - 4096, mid, 6, 1 << 32, 1, seqs=list(range(2, 100, 8)))
     job, hi = plant_job(oracle, job, mid, mid + 4096, 6, 1 << 32, 1, seqs=list(range(6, 100, 8)))
@@ -121,9 +122,9 @@ def test_config2_job_planted_across_2_51_and_at_2_62(sieve, oracle, rs):
 
 
 def test_config2_job_planted_across_3_2_49(sieve, oracle, rs):
-    """Planted factors on both sides of 3*2^49, where the set-up's chi chains
-    change from FP64 products (largest quotient error just below it) to lazy
-    Montgomery products."""
+    """Planted factors on both sides of 3*2^49, where the FP64 products of the
+    set-up's chi chains change from a quotient by h/p (largest error just
+    below it) to one by (h + l)/p."""
     mid = 3 << 49
     job, lo = plant_job(oracle, W.config2(2), mid - 8192, mid, 6, 1 << 32, 1, seqs=list(range(1, 100, 8)))
     job, hi = plant_job(oracle, job, mid, mid + 8192, 6, 1 << 32, 1, seqs=list(range(5, 100, 8)))
