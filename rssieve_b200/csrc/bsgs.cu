@@ -195,7 +195,7 @@ __shared__ u32 s_nsol, s_sol_i[KMAX], s_sol_u0[KMAX];   // small-order solutions
 // A residue's table value: the residue itself, or with FP64 steps (MODE 2) the
 // bit pattern of the double that holds it exactly (every step of that mode
 // yields canonical residues, so equal residues have equal bits).
-__device__ __forceinline__ u64 fp_val(u64 v) { return (u64)__double_as_longlong((double)v); }
+__device__ __forceinline__ u64 fp_val(u64 v) { return (u64)__double_as_longlong(fp_exact(v)); }
 __device__ __forceinline__ u64 fp_res(u64 bits) { return (u64)__longlong_as_double((long long)bits); }
 __device__ __forceinline__ u64 to_val(u64 v) { return s_ctx.fp ? fp_val(v) : v; }
 __device__ __forceinline__ u64 to_res(u64 val) { return s_ctx.fp ? fp_res(val) : val; }
@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             const u32 half = cp >> 1;
             u64 xa = x0, xb = mmul(x0, R.hdr.u2, p, q);
             if (MODE == 2) { xa = fp_val(xa); xb = fp_val(xb); }
-            const double pd = (double)p, sd = (double)sp, sq = __longlong_as_double((long long)R.hdr.S);
+            const double pd = fp_exact(p), sd = fp_exact(sp), sq = __longlong_as_double((long long)R.hdr.S);
             // IB2 values of each chain are hashed and stepped, then inserted, per
             // round (IB2 = IBMAX/2, or cp/2 when it is smaller)
             auto babies = [&](auto kind, auto ibc) {
@@ -612,7 +612,7 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                 // quotient constant), else the Montgomery product by S.
                 const u32 numk = R.hdr.numk, G = R.hdr.G, Lc = R.hdr.Lc;
                 const u64 S = R.hdr.S, Sw = R.hdr.Sw, Sp = R.hdr.Sp;
-                const double pd = (double)p, Sd = (double)Sp, Sqd = __longlong_as_double((long long)R.hdr.Sq);
+                const double pd = fp_exact(p), Sd = fp_exact(Sp), Sqd = __longlong_as_double((long long)R.hdr.Sq);
                 if (tid < numk * G) {
                     const u32 i = tid / G, g = tid - i * G;
                     const u32 q0 = g * Lc;

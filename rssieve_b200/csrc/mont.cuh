@@ -102,6 +102,13 @@ RS_DEV double fp_mul(double x, double y, double p, double pinv)
     return (r < 0.0) ? r + p : r;
 }
 
+// The double equal to v < 2^52, without a conversion instruction: v in the
+// mantissa of 2^52 + v (exponent field 0x433), then 2^52 subtracted exactly.
+RS_DEV double fp_exact(u64 v)
+{
+    return __longlong_as_double((long long)(0x4330000000000000ull | v)) - 4503599627370496.0;
+}
+
 // 2x mod p for x in [0, p), p < 2^52: exact in FP64.
 RS_DEV double fp_dbl(double x, double p)
 {

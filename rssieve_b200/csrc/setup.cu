@@ -54,7 +54,7 @@ struct PrimeAux {        // kernel 1 -> kernel 2 scalars
     u64 bm;              // Montgomery b
     u64 xD;              // (p-1)/D: chi(x) = x^xD
     u64 xe;              // eo/e
-    u64 h;               // Montgomery chi(b)^xe, of order e
+    u64 hm1;             // Montgomery h^-1, h = chi(b)^xe of order e
     u64 wr0[NCP];        // per baby-step count Q'_k = tpb*(C >> k): b^(nmin + e(Q'_k - 1)) * R^2 (mod p)
     u64 S[NCP];          //   and Montgomery s^Q'_k
     u32 e;               // split modulus
@@ -134,7 +134,7 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
     X.bm = bm;
     X.xD = xD;
     X.xe = xe;
-    X.h = mpow_call(gb, xe, M);
+    X.hm1 = mpow_call(mpow_call(gb, xe, M), (u64)(e - 1), M);
     X.e = e;
     const bool chi_m1 = (xD & 1) != 0;                    // chi(-1) = (-1)^xD
     X.flags = ((chi_m1 && (eo & 1)) ? AUX_NEG_EO : 0u) | ((chi_m1 && (xe & 1)) ? AUX_NEG_XE : 0u);
@@ -345,12 +345,35 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     const u64 mone = p - M.one;
     u64 *tg = tgt + (size_t)w * KSTRIDE;
     unsigned short *mg_ = meta + (size_t)w * KSTRIDE;
-    // hinv[r] = h^(-r) = h^((e - r) mod e) and, for now, wt[r] = b^r, for r < e
+    // hinv[r] = h^(-r) and, for now, wt[r] = b^r, for r < e: lane l forms
+    // h^(-l) and b^l by a multiplicative scan over the warp (five products
+    // each); entries 32..63 take one more product by h^(-32) and b^32
+    static_assert(SPLIT_MAX <= 64, "two rounds of 32 table entries");
     u64 *hinv = tw, *wt = tw + SPLIT_MAX;
     __syncwarp();                                          // the previous prime's readers are done
-    for (u32 r = lane; r < e; r += 32) {
-        hinv[r] = mpow_call(X.h, (u64)((e - r) % e), M);
-        wt[r] = mpow_call(X.bm, (u64)r, M);
+    {
+        const u64 hm1 = X.hm1, bm = X.bm;
+        u64 hv = (lane == 0) ? M.one : hm1, bv = (lane == 0) ? M.one : bm;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u64 hu = __shfl_up_sync(0xFFFFFFFFu, hv, o), bu = __shfl_up_sync(0xFFFFFFFFu, bv, o);
+            if (lane >= (u32)o) {
+                hv = mmul(hv, hu, p, M.q);
+                bv = mmul(bv, bu, p, M.q);
+            }
+        }
+        if (lane < e) {
+            hinv[lane] = hv;
+            wt[lane] = bv;
+        }
+        if (e > 32) {
+            const u64 h32 = mmul(__shfl_sync(0xFFFFFFFFu, hv, 31), hm1, p, M.q);
+            const u64 b32 = mmul(__shfl_sync(0xFFFFFFFFu, bv, 31), bm, p, M.q);
+            if (lane + 32 < e) {
+                hinv[lane + 32] = mmul(hv, h32, p, M.q);
+                wt[lane + 32] = mmul(bv, b32, p, M.q);
+            }
+        }
     }
     // z = chi(k) = k^xD for the lane's sequences i = lane + 32r, r < R: one
     // exponent for the whole warp, R independent chains per lane
