@@ -67,37 +67,45 @@ RS_DEV u64 msqr_lazy(u64 a, u64 p, u64 q)
     return hi + p - __umul64hi(t, p);
 }
 
+// round(a*b + c) - c for the exact product a*b, with c = 1.5*2^52: the fma
+// rounds once into [2^52, 2^53), where the doubles are the integers, so this
+// is a*b rounded to the nearest integer (ties to even) for |a*b| < 2^51, on
+// the FP64 pipe (rint would run on the slower conversion unit).
+RS_DEV double fp_round_prod(double a, double b)
+{
+    const double c = 6755399441055744.0;
+    return fma(a, b, c) - c;
+}
+
 // x*w mod p on the FP64 pipe, for p < 2^51 and x, w in [0, p) held exactly in
 // doubles, with wq = w/p (correctly rounded).  h = x*w rounded and the exact
 // error l = fma(x, w, -h) (the two-product of Dekker and Kahan's FMA form) give
-// x*w = h + l.  q = rint(x*wq) is within 1 of t = x*w/p: x*wq carries two
-// roundings, a relative error below 2^-52, i.e. below 1/2 since t < p < 2^51.
-// So r = x*w - q*p lies in (-p, p); it is formed exactly, since h - q*p is an
-// integer below 2^53 in magnitude (one fma) and adding l stays below 2^53.
-// One correction makes it canonical.  About eight FP64 operations, against
-// eighteen integer ones for Shoup's product.
+// x*w = h + l.  q, the exact product x*wq rounded to an integer, is within 1 of
+// t = x*w/p: wq carries one rounding, a relative error below 2^-53, i.e. below
+// 1/4 since t < p < 2^51, and the rounding adds at most 1/2.  So r = x*w - q*p
+// lies in (-p, p); it is formed exactly, since h - q*p is an integer below
+// 2^53 in magnitude (one fma) and adding l stays below 2^53.  One correction
+// makes it canonical.  About eight FP64 operations, against eighteen integer
+// ones for Shoup's product.
 RS_DEV double fp_mulfix(double x, double w, double wq, double p)
 {
     const double h = x * w;
     const double l = fma(x, w, -h);
-    const double q = rint(x * wq);
+    const double q = fp_round_prod(x, wq);
     const double r = fma(-q, p, h) + l;
     return (r < 0.0) ? r + p : r;
 }
 
-// x*y mod p on the FP64 pipe for two variable factors, with pinv = 1/p: as
-// fp_mulfix, but the quotient comes from pinv.  rint(h*pinv) carries three
-// roundings (h, pinv, the product), a relative error below 3*2^-53, which
-// stays below 1/2 for t = x*y/p < p < 3*2^49.  WIDE (p < 2^51) forms the
-// quotient as fma(h, pinv, l*pinv), i.e. from the exact h + l: two roundings
-// that matter (pinv, the fma; l*pinv is below 2^-2 in magnitude), a relative
-// error below 2^-52, below 1/2 for t < 2^51.  Either way r lies in (-p, p).
-template <bool WIDE = false>
+// x*y mod p on the FP64 pipe for two variable factors, p < 2^51, with pinv =
+// 1/p: as fp_mulfix, with the quotient from the exact product h*pinv rounded
+// to an integer.  h and pinv carry one rounding each, a relative error below
+// 2^-52, i.e. below 1/2 for t = x*y/p < 2^51, so again q is within 1 of t and
+// r lies in (-p, p).
 RS_DEV double fp_mul(double x, double y, double p, double pinv)
 {
     const double h = x * y;
     const double l = fma(x, y, -h);
-    const double q = rint(WIDE ? fma(h, pinv, l * pinv) : h * pinv);
+    const double q = fp_round_prod(h, pinv);
     const double r = fma(-q, p, h) + l;
     return (r < 0.0) ? r + p : r;
 }

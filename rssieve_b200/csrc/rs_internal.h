@@ -115,9 +115,7 @@ struct JobDev {
 // multiplier w takes its quotient from the double w/p.
 constexpr u64 FP_BOUND = 1ull << 51;
 // The set-up's chi chains (products of two variable factors, fp_mul) run on
-// the FP64 pipe below FP_BOUND as well, with a shorter quotient below
-// FP_MUL_BOUND = 3*2^49.
-constexpr u64 FP_MUL_BOUND = 3ull << 49;
+// the FP64 pipe below FP_BOUND as well.
 
 struct PrimeHdr {        // 128 bytes (a 16-byte multiple: copied by TMA bulk copies)
     u64 p;               // 0 = skipped

@@ -249,37 +249,35 @@ __device__ __forceinline__ void mpow_lanes(u32 R, u64 (&a)[4], const u64 (&x)[4]
 }
 
 // The chains of mpow_multi on the FP64 pipe (p < FP_BOUND): plain residues
-// held exactly in doubles, products by fp_mul (its WIDE quotient from
-// FP_MUL_BOUND on).
-template <int R, bool WIDE>
+// held exactly in doubles, products by fp_mul.
+template <int R>
 __device__ __forceinline__ void fpow_multi(double (&a)[4], const double (&x)[4], u64 ex, double pd, double pinv)
 {
 #pragma unroll
     for (int r = 0; r < R; ++r) a[r] = x[r];
     for (int bit = 62 - __clzll(ex); bit >= 0; --bit) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[r] = fp_mul<WIDE>(a[r], a[r], pd, pinv);
+        for (int r = 0; r < R; ++r) a[r] = fp_mul(a[r], a[r], pd, pinv);
         if ((ex >> bit) & 1) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) a[r] = fp_mul<WIDE>(a[r], x[r], pd, pinv);
+            for (int r = 0; r < R; ++r) a[r] = fp_mul(a[r], x[r], pd, pinv);
         }
     }
 }
 
 // At most two chains at a time: FP64 products have short enough latencies,
 // and four interleaved chains would not fit the kernel's 64 registers.
-template <bool WIDE>
 __device__ __forceinline__ void fpow_lanes(u32 R, double (&a)[4], const double (&x)[4], u64 ex, double pd, double pinv)
 {
     if (R == 1) {
-        fpow_multi<1, WIDE>(a, x, ex, pd, pinv);
+        fpow_multi<1>(a, x, ex, pd, pinv);
         return;
     }
-    fpow_multi<2, WIDE>(a, x, ex, pd, pinv);
+    fpow_multi<2>(a, x, ex, pd, pinv);
     if (R > 2) {
         double a2[4], x2[4] = {x[2], x[3], x[3], x[3]};
-        if (R == 3) fpow_multi<1, WIDE>(a2, x2, ex, pd, pinv);
-        else fpow_multi<2, WIDE>(a2, x2, ex, pd, pinv);
+        if (R == 3) fpow_multi<1>(a2, x2, ex, pd, pinv);
+        else fpow_multi<2>(a2, x2, ex, pd, pinv);
         a[2] = a2[0];
         a[3] = a2[1];
     }
@@ -305,8 +303,7 @@ __device__ __forceinline__ Chi4 chi_of_ks(const JobDev *__restrict__ job, u32 la
             x[r] = (double)((kv < p) ? kv : kv % p);
         }
         const double pd = (double)p;
-        if (p < FP_MUL_BOUND) fpow_lanes<false>(R, zd, x, xD, pd, 1.0 / pd);
-        else fpow_lanes<true>(R, zd, x, xD, pd, 1.0 / pd);
+        fpow_lanes(R, zd, x, xD, pd, 1.0 / pd);
 #pragma unroll
         for (int r = 0; r < 4; ++r) out.z[r] = to_mont((u64)zd[r], M);
     } else {

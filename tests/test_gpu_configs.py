@@ -122,9 +122,8 @@ def test_config2_job_planted_across_2_51_and_at_2_62(sieve, oracle, rs):
 
 
 def test_config2_job_planted_across_3_2_49(sieve, oracle, rs):
-    """Planted factors on both sides of 3*2^49, where the FP64 products of the
-    set-up's chi chains change from a quotient by h/p (largest error just
-    below it) to one by (h + l)/p."""
+    """Planted factors on both sides of 3*2^49, three quarters of the way to
+    the 2^51 bound of the FP64 products (chi chains, baby and giant steps)."""
     mid = 3 << 49
     job, lo = plant_job(oracle, W.config2(2), mid - 8192, mid, 6, 1 << 32, 1, seqs=list(range(1, 100, 8)))
     job, hi = plant_job(oracle, job, mid, mid + 8192, 6, 1 << 32, 1, seqs=list(range(5, 100, 8)))
