@@ -356,7 +356,9 @@ __device__ __noinline__ void small_order_search(const RecBuf *R, u32 order)
     const u64 *st = Smem<TPB, NB>::start();
     const u32 tid = threadIdx.x;
     if (tid < R->hdr.numk) {
-        const u64 Tv = to_val(R->tgt[tid]);
+        // FP64 launches' tables carry R^2: the target T*R times R^2 mod p
+        // (the header's ssw there) by one Montgomery product
+        const u64 Tv = to_val(s_ctx.fp ? mmul(R->tgt[tid], R->hdr.ssw, s_ctx.p, s_ctx.q) : R->tgt[tid]);
         u32 b, fp;
         tab_hash<NB>(Tv, b, fp);
         for (int pr = 0; pr < BSGS_MAXPROBE; ++pr) {
@@ -505,15 +507,26 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                 fetch(buf ^ 1, nxt);
             }
         }
+        // MODE 2: start values by FP64 products x*y mod p (1/p in the header's
+        // Sw), the set-up having stored Z2, s^(cp/2) and S^(Lc/2) plain: baby and
+        // giant values carry R^2 (the header's ssw) where the integer modes'
+        // Montgomery products leave R
+        const double pd = fp_exact(p), pinv = __longlong_as_double((long long)R.hdr.Sw);
         if (live) {
-            if (tid < R.hdr.G) s_Z[tid] = mmul(R.tabs[64 + (tid & 31)], R.tabs[96 + (tid >> 5)], p, q);
+            if (tid < R.hdr.G) {
+                const u64 z1 = R.tabs[64 + (tid & 31)], z2 = R.tabs[96 + (tid >> 5)];
+                s_Z[tid] = (MODE == 2) ? (u64)__double_as_longlong(fp_mul(fp_exact(z1), fp_exact(z2), pd, pinv))
+                                       : mmul(z1, z2, p, q);
+            }
             // ---- baby steps y_j = s^j, j < Q' = TPB*cp, inserted as they are produced ----
             // Speculative: ord(s) < Q' is only known after the barrier; then the
             // table (which may hold repeats) is rebuilt from j < ord.
-            const u64 x0 = mmul(R.tabs[tid & 31], R.tabs[32 + (tid >> 5)], p, q);   // s^(cp*tid)
-            // MODE 2: table values are the bits of the doubles holding the residues
-            const u64 one = (MODE == 2) ? fp_val(R.hdr.one) : R.hdr.one;
-            s_start[tid] = (MODE == 2) ? fp_val(x0) : x0;
+            const u64 ta = R.tabs[tid & 31], tb = R.tabs[32 + (tid >> 5)];
+            // s^(cp*tid); MODE 2: table values are the bits of the doubles holding the residues
+            const u64 x0 = (MODE == 2) ? (u64)__double_as_longlong(fp_mul(fp_exact(ta), fp_exact(tb), pd, pinv))
+                                       : mmul(ta, tb, p, q);
+            const u64 one = (MODE == 2) ? fp_val(R.hdr.ssw) : R.hdr.one;
+            s_start[tid] = x0;
             u32 spill = 0;
             // Two chains per thread, j in [tid*cp, tid*cp + cp/2) and the next
             // cp/2 (started from s^(cp/2) further), so the two products of a step
@@ -527,9 +540,12 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
             const u64 ssw = R.hdr.ssw;
             const u64 sp = R.hdr.sp;
             const u32 half = cp >> 1;
-            u64 xa = x0, xb = mmul(x0, R.hdr.u2, p, q);
-            if (MODE == 2) { xa = fp_val(xa); xb = fp_val(xb); }
-            const double pd = fp_exact(p), sd = fp_exact(sp), sq = __longlong_as_double((long long)R.hdr.S);
+            u64 xa = x0, xb;
+            if (MODE == 2)
+                xb = (u64)__double_as_longlong(fp_mul(__longlong_as_double((long long)x0), fp_exact(R.hdr.u2), pd, pinv));
+            else
+                xb = mmul(x0, R.hdr.u2, p, q);
+            const double sd = fp_exact(sp), sq = __longlong_as_double((long long)R.hdr.S);
             // IB2 values of each chain are hashed and stepped, then inserted, per
             // round (IB2 = IBMAX/2, or cp/2 when it is smaller)
             auto babies = [&](auto kind, auto ibc) {
@@ -612,17 +628,26 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) k_bsgs(BsgsArgs a, const Prim
                 // quotient constant), else the Montgomery product by S.
                 const u32 numk = R.hdr.numk, G = R.hdr.G, Lc = R.hdr.Lc;
                 const u64 S = R.hdr.S, Sw = R.hdr.Sw, Sp = R.hdr.Sp;
-                const double pd = fp_exact(p), Sd = fp_exact(Sp), Sqd = __longlong_as_double((long long)R.hdr.Sq);
+                const double Sd = fp_exact(Sp), Sqd = __longlong_as_double((long long)R.hdr.Sq);
                 if (tid < numk * G) {
-                    const u32 i = tid / G, g = tid - i * G;
+                    // i = tid / G by a float reciprocal: (tid + 1/2) / G lies at
+                    // least 1/(2G) from an integer, and the two roundings err by
+                    // under 2^-22 relative (below 2^-12 * (1024/G) absolute)
+                    const u32 i = (u32)(((float)tid + 0.5f) * __frcp_rn((float)G)), g = tid - i * G;
                     const u32 q0 = g * Lc;
                     const u32 q1 = min(q0 + Lc, Mg);
                     const u32 h = Lc >> 1;
                     const u32 nA = min(h, q1 - q0), nB = (q1 - q0) - nA;
                     const u32 m = R.meta[i];
-                    u64 gA = mmul(R.tgt[i], s_Z[g], p, q);
-                    u64 gB = mmul(gA, R.hdr.Sh, p, q);
-                    if (MODE == 2) { gA = fp_val(gA); gB = fp_val(gB); }
+                    u64 gA, gB;
+                    if (MODE == 2) {
+                        const double a0 = fp_mul(fp_exact(R.tgt[i]), __longlong_as_double((long long)s_Z[g]), pd, pinv);
+                        gA = (u64)__double_as_longlong(a0);
+                        gB = (u64)__double_as_longlong(fp_mul(a0, fp_exact(R.hdr.Sh), pd, pinv));
+                    } else {
+                        gA = mmul(R.tgt[i], s_Z[g], p, q);
+                        gB = mmul(gA, R.hdr.Sh, p, q);
+                    }
                     auto gstep = [&](u64 v) -> u64 {
                         if (MODE == 2)
                             return (u64)__double_as_longlong(fp_mulfix(__longlong_as_double((long long)v), Sd, Sqd, pd));

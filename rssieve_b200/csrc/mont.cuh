@@ -110,6 +110,18 @@ RS_DEV double fp_mul(double x, double y, double p, double pinv)
     return (r < 0.0) ? r + p : r;
 }
 
+// fp_mul without its correction, for chains of products: for x, y in (-p, p)
+// the bounds above hold unchanged (|x*y| < p^2, so |t| < p and q is within 1
+// of t), hence r = x*y - q*p is exact and lies in (-p, p) again.  A chain
+// stays in signed residues and is made canonical once at its end.
+RS_DEV double fp_mul_signed(double x, double y, double p, double pinv)
+{
+    const double h = x * y;
+    const double l = fma(x, y, -h);
+    const double q = fp_round_prod(h, pinv);
+    return fma(-q, p, h) + l;
+}
+
 // The double equal to v < 2^52, without a conversion instruction: v in the
 // mantissa of 2^52 + v (exponent field 0x433), then 2^52 subtracted exactly.
 RS_DEV double fp_exact(u64 v)

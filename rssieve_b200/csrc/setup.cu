@@ -249,7 +249,8 @@ __device__ __forceinline__ void mpow_lanes(u32 R, u64 (&a)[4], const u64 (&x)[4]
 }
 
 // The chains of mpow_multi on the FP64 pipe (p < FP_BOUND): plain residues
-// held exactly in doubles, products by fp_mul.
+// held exactly in doubles, products by fp_mul_signed, so the chains run in
+// signed residues in (-p, p) and are made canonical once at the end.
 template <int R>
 __device__ __forceinline__ void fpow_multi(double (&a)[4], const double (&x)[4], u64 ex, double pd, double pinv)
 {
@@ -257,12 +258,14 @@ __device__ __forceinline__ void fpow_multi(double (&a)[4], const double (&x)[4],
     for (int r = 0; r < R; ++r) a[r] = x[r];
     for (int bit = 62 - __clzll(ex); bit >= 0; --bit) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) a[r] = fp_mul(a[r], a[r], pd, pinv);
+        for (int r = 0; r < R; ++r) a[r] = fp_mul_signed(a[r], a[r], pd, pinv);
         if ((ex >> bit) & 1) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) a[r] = fp_mul(a[r], x[r], pd, pinv);
+            for (int r = 0; r < R; ++r) a[r] = fp_mul_signed(a[r], x[r], pd, pinv);
         }
     }
+#pragma unroll
+    for (int r = 0; r < R; ++r) a[r] = (a[r] < 0.0) ? a[r] + pd : a[r];
 }
 
 // At most two chains at a time: FP64 products have short enough latencies,
@@ -320,13 +323,52 @@ __device__ __forceinline__ Chi4 chi_of_ks(const JobDev *__restrict__ job, u32 la
     return out;
 }
 
+// Class lookup: the e values h^(-r) (r < e <= SPLIT_MAX, all distinct and
+// nonzero) in an open-addressed table of CLS_SLOTS 64-bit keys with their r
+// beside them, so a sequence's class costs one or two probes instead of a
+// walk over up to e entries (e averages about 28 at 2^50).
+constexpr u32 CLS_SLOTS = 2 * SPLIT_MAX;
+static_assert((CLS_SLOTS & (CLS_SLOTS - 1)) == 0, "slot index wraps by a mask");
+
+__device__ __forceinline__ u32 cls_hash(u64 v) { return (((u32)v ^ (u32)(v >> 32)) * 0x9E3779B1u) >> 25; }
+static_assert(CLS_SLOTS == 128, "cls_hash yields 7 bits");
+
+// Inserts key v (nonzero, not yet present) with index r; lanes insert
+// concurrently, a slot going to the lane whose compare-and-swap finds it empty.
+// At most SPLIT_MAX keys share CLS_SLOTS slots, so the walk always ends.
+__device__ __forceinline__ void cls_insert(u64 *ck, unsigned char *cr, u64 v, u32 r)
+{
+    u32 s = cls_hash(v);
+    for (u32 n = 0; n < CLS_SLOTS; ++n) {
+        if (atomicCAS(reinterpret_cast<unsigned long long *>(&ck[s]), 0ull, (unsigned long long)v) == 0ull) {
+            cr[s] = (unsigned char)r;
+            return;
+        }
+        s = (s + 1) & (CLS_SLOTS - 1);
+    }
+}
+
+// r with ck[.] == v, or none when v is absent (an empty slot ends the walk).
+__device__ __forceinline__ u32 cls_find(const u64 *ck, const unsigned char *cr, u64 v, u32 none)
+{
+    u32 s = cls_hash(v);
+    for (u32 n = 0; n < CLS_SLOTS; ++n) {
+        const u64 k = ck[s];
+        if (k == v) return cr[s];
+        if (k == 0) break;
+        s = (s + 1) & (CLS_SLOTS - 1);
+    }
+    return none;
+}
+
 // Sequence classes, targets, baby-step count and the start tables of record w
-// (one warp).  tw: this warp's two tables of SPLIT_MAX entries in shared memory.
+// (one warp).  tw: this warp's table of SPLIT_MAX powers of b followed by the
+// CLS_SLOTS keys of its class lookup; cr: the lookup's indices.
 __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 w, u32 lane, PrimeHdr *__restrict__ hdr,
                                             const PrimeAux *__restrict__ aux, u64 *__restrict__ tabs,
                                             u64 *__restrict__ tgt, unsigned short *__restrict__ meta,
                                             u64 *__restrict__ stats, u32 *__restrict__ err, const JobGeom &gm,
-                                            u64 *tw)
+                                            u64 *tw, unsigned char *cr)
 {
     PrimeHdr H = hdr[w];
     if (H.p == 0) {
@@ -342,12 +384,15 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     const u64 mone = p - M.one;
     u64 *tg = tgt + (size_t)w * KSTRIDE;
     unsigned short *mg_ = meta + (size_t)w * KSTRIDE;
-    // hinv[r] = h^(-r) and, for now, wt[r] = b^r, for r < e: lane l forms
-    // h^(-l) and b^l by a multiplicative scan over the warp (five products
-    // each); entries 32..63 take one more product by h^(-32) and b^32
+    // the class lookup gets h^(-r) and, for now, wt[r] = b^r, for r < e: lane
+    // l forms h^(-l) and b^l by a multiplicative scan over the warp (five
+    // products each); entries 32..63 take one more product by h^(-32) and b^32
     static_assert(SPLIT_MAX <= 64, "two rounds of 32 table entries");
-    u64 *hinv = tw, *wt = tw + SPLIT_MAX;
+    u64 *wt = tw, *ck = tw + SPLIT_MAX;
     __syncwarp();                                          // the previous prime's readers are done
+#pragma unroll
+    for (u32 i = 0; i < CLS_SLOTS; i += 32) ck[i + lane] = 0;
+    __syncwarp();
     {
         const u64 hm1 = X.hm1, bm = X.bm;
         u64 hv = (lane == 0) ? M.one : hm1, bv = (lane == 0) ? M.one : bm;
@@ -360,14 +405,14 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
             }
         }
         if (lane < e) {
-            hinv[lane] = hv;
+            cls_insert(ck, cr, hv, lane);
             wt[lane] = bv;
         }
         if (e > 32) {
             const u64 h32 = mmul(__shfl_sync(0xFFFFFFFFu, hv, 31), hm1, p, M.q);
             const u64 b32 = mmul(__shfl_sync(0xFFFFFFFFu, bv, 31), bm, p, M.q);
             if (lane + 32 < e) {
-                hinv[lane + 32] = mmul(hv, h32, p, M.q);
+                cls_insert(ck, cr, mmul(hv, h32, p, M.q), lane + 32);
                 wt[lane + 32] = mmul(bv, b32, p, M.q);
             }
         }
@@ -405,13 +450,11 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
                 const u64 want = (ci == 1 && (X.flags & AUX_NEG_EO)) ? mone : M.one;
                 const bool pass = (X.xe == 1) || mpow_call(z1, (u64)e, M) == want;
                 if (pass) {
-                    // n == r (mod e) where z1 * h^r == chi(-c)^xe
+                    // n == r (mod e) where z1 * h^r == chi(-c)^xe, i.e.
+                    // h^(-r) == z1 or, when chi(-c)^xe == -1, == p - z1
+                    // (z1 is a unit, so both lie in (0, p))
                     const bool neg = (ci == 1) && (X.flags & AUX_NEG_XE);
-                    u32 r = e;
-                    for (u32 rr = 0; rr < e; ++rr) {
-                        const u64 hv = hinv[rr];
-                        if (z1 == (neg ? p - hv : hv)) { r = rr; break; }
-                    }
+                    const u32 r = cls_find(ck, cr, neg ? p - z1 : z1, e);
                     if (r < e) {
                         const u32 off = (r + e - nmod) % e;
                         mt = (unsigned short)(i | (off << 7));
@@ -498,8 +541,13 @@ __device__ __forceinline__ void setup_tabs_one(const JobDev *__restrict__ job, u
         b = mmul(b, z, p, q);
     }
     const u64 u32p = a, z32 = b;                           // u^32, z^32
+    // Below FP_BOUND the BSGS kernel forms its start values with FP64 products
+    // of plain residues, x*y mod p instead of x*y/R: there Z2, s^(cp/2) and
+    // S^(Lc/2) are stored plain (Z2 by starting its chain at 1 instead of R),
+    // so baby and giant values alike carry R^2 instead of R.
+    const bool fp = (p < FP_BOUND);
     a = M.one;
-    b = M.one;
+    b = fp ? 1u : M.one;
     for (int l = 0; l < 32; ++l) {
         tb[32 + l] = a;
         tb[96 + l] = b;
@@ -517,10 +565,16 @@ __device__ __forceinline__ void setup_tabs_one(const JobDev *__restrict__ job, u
         h.Sp = from_mont(S, M);
         h.Sw = shoup_of_mont(S, q);
     }
-    if (p < FP_BOUND) {                                    // FP64 quotients of the baby and giant multipliers
+    if (fp) {                                              // FP64 quotients of the baby and giant multipliers
         const double pd = (double)p;
         h.S = (u64)__double_as_longlong((double)H.sp / pd);
         h.Sq = (u64)__double_as_longlong((double)h.Sp / pd);
+        // the FP64 start values: plain s^(cp/2) and S^(Lc/2), 1/p in the Shoup
+        // quotients' place and R^2 mod p (the value of s^0) in the other
+        h.u2 = from_mont(u2, M);
+        h.Sh = from_mont(Sh, M);
+        h.Sw = (u64)__double_as_longlong(1.0 / pd);
+        h.ssw = aux[t].r2;
     }
     n_targets += nk;
     if (e >= 2) ++n_split; else ++n_full;
@@ -571,21 +625,23 @@ __global__ void __launch_bounds__(SETUP_TPB, 4) k_setup_k(const JobDev *__restri
                                                        const u32 *__restrict__ prefix, u32 nr,
                                                        const u32 *__restrict__ rec_of)
 {
-    __shared__ u64 s_tw[SETUP_TPB / 32][2 * SPLIT_MAX];   // per warp: class and target tables of its prime
+    __shared__ u64 s_tw[SETUP_TPB / 32][SPLIT_MAX + CLS_SLOTS];   // per warp: powers of b, class lookup keys
+    __shared__ unsigned char s_cr[SETUP_TPB / 32][CLS_SLOTS];     //   and the lookup's class indices
     const u32 lane = threadIdx.x & 31;
     const u32 nwarps = gridDim.x * (SETUP_TPB / 32);
     u64 *tw = s_tw[threadIdx.x >> 5];
+    unsigned char *cr = s_cr[threadIdx.x >> 5];
     // w is uniform over the warp, so the warp-wide ballots of a prime stay whole
     if constexpr (BATCH) {
         const u32 total = prefix[nr];
         for (u32 i = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5; i < total; i += nwarps) {
             const u32 rec = rec_of[i];
             const u32 jb = hdr[rec].job;
-            setup_k_one(jobs + jb, rec, lane, hdr, aux, tabs, tgt, meta, stats, err, geoms[jb], tw);
+            setup_k_one(jobs + jb, rec, lane, hdr, aux, tabs, tgt, meta, stats, err, geoms[jb], tw, cr);
         }
     } else {
         for (u32 w = (blockIdx.x * SETUP_TPB + threadIdx.x) >> 5; w < count; w += nwarps)
-            setup_k_one(jobs, w, lane, hdr, aux, tabs, tgt, meta, stats, err, gm, tw);
+            setup_k_one(jobs, w, lane, hdr, aux, tabs, tgt, meta, stats, err, gm, tw, cr);
     }
 }
 
