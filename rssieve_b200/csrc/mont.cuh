@@ -129,6 +129,13 @@ RS_DEV double fp_exact(u64 v)
     return __longlong_as_double((long long)(0x4330000000000000ull | v)) - 4503599627370496.0;
 }
 
+// The integer held by a double d in [0, 2^52), without a conversion
+// instruction: d + 2^52 puts it in the mantissa (exactly), which is masked out.
+RS_DEV u64 fp_int(double d)
+{
+    return (u64)__double_as_longlong(d + 4503599627370496.0) & ((1ull << 52) - 1);
+}
+
 // 2x mod p for x in [0, p), p < 2^52: exact in FP64.
 RS_DEV double fp_dbl(double x, double p)
 {

@@ -303,12 +303,12 @@ __device__ __forceinline__ Chi4 chi_of_ks(const JobDev *__restrict__ job, u32 la
         for (int r = 0; r < 4; ++r) {
             const u32 i = lane + 32 * r;
             const u64 kv = (i < K) ? job->k[i] : 1;
-            x[r] = (double)((kv < p) ? kv : kv % p);
+            x[r] = fp_exact((kv < p) ? kv : kv % p);
         }
         const double pd = (double)p;
         fpow_lanes(R, zd, x, xD, pd, 1.0 / pd);
 #pragma unroll
-        for (int r = 0; r < 4; ++r) out.z[r] = to_mont((u64)zd[r], M);
+        for (int r = 0; r < 4; ++r) out.z[r] = to_mont(fp_int(zd[r]), M);
     } else {
         u64 x[4];
 #pragma unroll
@@ -362,8 +362,9 @@ __device__ __forceinline__ u32 cls_find(const u64 *ck, const unsigned char *cr, 
 }
 
 // Sequence classes, targets, baby-step count and the start tables of record w
-// (one warp).  tw: this warp's table of SPLIT_MAX powers of b followed by the
-// CLS_SLOTS keys of its class lookup; cr: the lookup's indices.
+// (one warp).  tw: this warp's table of SPLIT_MAX powers of b, the CLS_SLOTS
+// keys of its class lookup and chi(k) of up to 128 sequences; cr: the
+// lookup's indices.
 __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 w, u32 lane, PrimeHdr *__restrict__ hdr,
                                             const PrimeAux *__restrict__ aux, u64 *__restrict__ tabs,
                                             u64 *__restrict__ tgt, unsigned short *__restrict__ meta,
@@ -388,7 +389,7 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     // l forms h^(-l) and b^l by a multiplicative scan over the warp (five
     // products each); entries 32..63 take one more product by h^(-32) and b^32
     static_assert(SPLIT_MAX <= 64, "two rounds of 32 table entries");
-    u64 *wt = tw, *ck = tw + SPLIT_MAX;
+    u64 *wt = tw, *ck = tw + SPLIT_MAX, *zs = ck + CLS_SLOTS;
     __syncwarp();                                          // the previous prime's readers are done
 #pragma unroll
     for (u32 i = 0; i < CLS_SLOTS; i += 32) ck[i + lane] = 0;
@@ -396,7 +397,7 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     {
         const u64 hm1 = X.hm1, bm = X.bm;
         u64 hv = (lane == 0) ? M.one : hm1, bv = (lane == 0) ? M.one : bm;
-#pragma unroll
+#pragma unroll 1
         for (int o = 1; o < 32; o <<= 1) {
             const u64 hu = __shfl_up_sync(0xFFFFFFFFu, hv, o), bu = __shfl_up_sync(0xFFFFFFFFu, bv, o);
             if (lane >= (u32)o) {
@@ -420,18 +421,24 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     // z = chi(k) = k^xD for the lane's sequences i = lane + 32r, r < R: one
     // exponent for the whole warp, R independent chains per lane
     const u32 R = (K + 31) / 32;
-    const Chi4 zc = chi_of_ks(job, lane, K, M, X.xD);
-    const u64 (&z)[4] = zc.z;
+    {
+        const Chi4 zc = chi_of_ks(job, lane, K, M, X.xD);
+#pragma unroll
+        for (u32 r = 0; r < 4; ++r)
+            if (r < R) zs[lane + 32 * r] = zc.z[r];
+    }
     __syncwarp();
     // pass 1: the class of every sequence; the kept ones' k mod p and class
-    // offset go to the record (compacted), the target itself once Q' is known
+    // offset go to the record (compacted), the target itself once Q' is known.
+    // The rounds read chi(k) back from shared memory, so the loop is not
+    // unrolled: one copy of its code keeps the kernel's hot path short.
     const u32 nmod = job->nmin % e;
     u32 nk = 0;
     bool divk = false, lost = false;
-#pragma unroll
-    for (int rd = 0; rd < 4; ++rd) {
-        if ((u32)rd >= R) break;
+#pragma unroll 1
+    for (u32 rd = 0; rd < R; ++rd) {
         const u32 i = lane + 32 * rd;
+        const u64 zr = zs[i];
         bool keep = false;
         u64 kr = 0;
         unsigned short mt = 0;
@@ -446,7 +453,7 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
                 // z1^e == chi(-c)^eo with z1 = z^xe; chi(-c) is 1 for c = -1.
                 // When xe = 1 (eo = e, the usual case) that is exactly "the class
                 // search below finds r", so the power is skipped.
-                const u64 z1 = (X.xe == 1) ? z[rd] : mpow_call(z[rd], X.xe, M);
+                const u64 z1 = (X.xe == 1) ? zr : mpow_call(zr, X.xe, M);
                 const u64 want = (ci == 1 && (X.flags & AUX_NEG_EO)) ? mone : M.one;
                 const bool pass = (X.xe == 1) || mpow_call(z1, (u64)e, M) == want;
                 if (pass) {
@@ -532,27 +539,49 @@ __device__ __forceinline__ void setup_tabs_one(const JobDev *__restrict__ job, u
     for (u32 c = cp >> 1; c > 1; c >>= 1) u2 = mmul(u2, u2, p, q);
     const u64 u = mmul(u2, u2, p, q);
     u64 *tb = tabs + (size_t)t * TABS;
-    // four power tables, two chains at a time
-    u64 a = M.one, b = M.one;
-    for (int l = 0; l < 32; ++l) {
-        tb[l] = a;
-        tb[64 + l] = b;
-        a = mmul(a, u, p, q);
-        b = mmul(b, z, p, q);
-    }
-    const u64 u32p = a, z32 = b;                           // u^32, z^32
-    // Below FP_BOUND the BSGS kernel forms its start values with FP64 products
-    // of plain residues, x*y mod p instead of x*y/R: there Z2, s^(cp/2) and
-    // S^(Lc/2) are stored plain (Z2 by starting its chain at 1 instead of R),
-    // so baby and giant values alike carry R^2 instead of R.
+    // four power tables, two chains at a time.  Below FP_BOUND the BSGS kernel
+    // forms its start values with FP64 products of plain residues, x*y mod p
+    // instead of x*y/R: there Z2, s^(cp/2) and S^(Lc/2) are stored plain, so
+    // baby and giant values alike carry R^2 instead of R; and the tables' own
+    // chains run on the FP64 pipe with plain multipliers (an R-form start
+    // times plain powers stays in R-form).
     const bool fp = (p < FP_BOUND);
-    a = M.one;
-    b = fp ? 1u : M.one;
-    for (int l = 0; l < 32; ++l) {
-        tb[32 + l] = a;
-        tb[96 + l] = b;
-        a = mmul(a, u32p, p, q);
-        b = mmul(b, z32, p, q);
+    if (fp) {
+        const double pd = (double)p, pinv = 1.0 / pd;
+        const double up = fp_exact(from_mont(u, M)), zp = fp_exact(from_mont(z, M));
+        double a = fp_exact(M.one), b = a;
+        for (int l = 0; l < 32; ++l) {
+            tb[l] = fp_int(a);
+            tb[64 + l] = fp_int(b);
+            a = fp_mul(a, up, pd, pinv);
+            b = fp_mul(b, zp, pd, pinv);
+        }
+        const double u32p = fp_exact(from_mont(fp_int(a), M)), z32 = fp_exact(from_mont(fp_int(b), M));   // plain u^32, z^32
+        a = fp_exact(M.one);
+        b = 1.0;
+        for (int l = 0; l < 32; ++l) {
+            tb[32 + l] = fp_int(a);
+            tb[96 + l] = fp_int(b);
+            a = fp_mul(a, u32p, pd, pinv);
+            b = fp_mul(b, z32, pd, pinv);
+        }
+    } else {
+        u64 a = M.one, b = M.one;
+        for (int l = 0; l < 32; ++l) {
+            tb[l] = a;
+            tb[64 + l] = b;
+            a = mmul(a, u, p, q);
+            b = mmul(b, z, p, q);
+        }
+        const u64 u32p = a, z32 = b;                       // u^32, z^32
+        a = M.one;
+        b = M.one;
+        for (int l = 0; l < 32; ++l) {
+            tb[32 + l] = a;
+            tb[96 + l] = b;
+            a = mmul(a, u32p, p, q);
+            b = mmul(b, z32, p, q);
+        }
     }
     PrimeHdr &h = hdr[t];
     h.G = G;
@@ -625,7 +654,7 @@ __global__ void __launch_bounds__(SETUP_TPB, 4) k_setup_k(const JobDev *__restri
                                                        const u32 *__restrict__ prefix, u32 nr,
                                                        const u32 *__restrict__ rec_of)
 {
-    __shared__ u64 s_tw[SETUP_TPB / 32][SPLIT_MAX + CLS_SLOTS];   // per warp: powers of b, class lookup keys
+    __shared__ u64 s_tw[SETUP_TPB / 32][SPLIT_MAX + CLS_SLOTS + 4 * 32];   // per warp: powers of b, class lookup keys, chi(k)
     __shared__ unsigned char s_cr[SETUP_TPB / 32][CLS_SLOTS];     //   and the lookup's class indices
     const u32 lane = threadIdx.x & 31;
     const u32 nwarps = gridDim.x * (SETUP_TPB / 32);
