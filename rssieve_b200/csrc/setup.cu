@@ -79,6 +79,26 @@ __device__ __forceinline__ void order_step(u64 &eo, u64 g, const Mont &M)
     while (eo % L == 0 && mpow_call(g, eo / L, M) == M.one) eo /= L;
 }
 
+// x^e mod p on the FP64 pipe (p < FP_BOUND), plain residues held exactly in
+// doubles, pinv = 1/p; e may be 0.  Out of line like mpow_call.
+__device__ __noinline__ double fpow_call(double x, u64 e, double p, double pinv)
+{
+    if (e == 0) return 1.0;
+    double a = x;
+    for (int bit = 62 - __clzll(e); bit >= 0; --bit) {
+        a = fp_mul(a, a, p, pinv);
+        if ((e >> bit) & 1) a = fp_mul(a, x, p, pinv);
+    }
+    return a;
+}
+
+// order_step for a plain g below FP_BOUND, by FP64 powers.
+template <u32 L>
+__device__ __forceinline__ void order_step_fp(u64 &eo, double g, double p, double pinv)
+{
+    while (eo % L == 0 && fpow_call(g, eo / L, p, pinv) == 1.0) eo /= L;
+}
+
 // Largest divisor of eo that is at most SPLIT_MAX.
 __device__ __forceinline__ u32 split_modulus(u64 eo)
 {
@@ -119,13 +139,25 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
     strip<13>(xD, D); strip<17>(xD, D); strip<19>(xD, D); strip<23>(xD, D); strip<29>(xD, D);
     strip<31>(xD, D); strip<37>(xD, D); strip<41>(xD, D); strip<43>(xD, D); strip<47>(xD, D);
     strip<53>(xD, D); strip<59>(xD, D); strip<61>(xD, D);
-    const u64 gb = mpow(bm, xD, M);                       // chi(b), of order eo | D
-    u64 eo = D;
-    order_step<2>(eo, gb, M);  order_step<3>(eo, gb, M);  order_step<5>(eo, gb, M);  order_step<7>(eo, gb, M);
-    order_step<11>(eo, gb, M); order_step<13>(eo, gb, M); order_step<17>(eo, gb, M); order_step<19>(eo, gb, M);
-    order_step<23>(eo, gb, M); order_step<29>(eo, gb, M); order_step<31>(eo, gb, M); order_step<37>(eo, gb, M);
-    order_step<41>(eo, gb, M); order_step<43>(eo, gb, M); order_step<47>(eo, gb, M); order_step<53>(eo, gb, M);
-    order_step<59>(eo, gb, M); order_step<61>(eo, gb, M);
+    u64 gb, eo = D;                                       // chi(b), of order eo | D
+    if (p < FP_BOUND) {                                   // the power and the order on the FP64 pipe
+        const double pd = fp_exact(p), pinv = 1.0 / pd;
+        const double g = fpow_call(fp_exact(b % p), xD, pd, pinv);
+        order_step_fp<2>(eo, g, pd, pinv);  order_step_fp<3>(eo, g, pd, pinv);  order_step_fp<5>(eo, g, pd, pinv);
+        order_step_fp<7>(eo, g, pd, pinv);  order_step_fp<11>(eo, g, pd, pinv); order_step_fp<13>(eo, g, pd, pinv);
+        order_step_fp<17>(eo, g, pd, pinv); order_step_fp<19>(eo, g, pd, pinv); order_step_fp<23>(eo, g, pd, pinv);
+        order_step_fp<29>(eo, g, pd, pinv); order_step_fp<31>(eo, g, pd, pinv); order_step_fp<37>(eo, g, pd, pinv);
+        order_step_fp<41>(eo, g, pd, pinv); order_step_fp<43>(eo, g, pd, pinv); order_step_fp<47>(eo, g, pd, pinv);
+        order_step_fp<53>(eo, g, pd, pinv); order_step_fp<59>(eo, g, pd, pinv); order_step_fp<61>(eo, g, pd, pinv);
+        gb = to_mont(fp_int(g), M);
+    } else {
+        gb = mpow(bm, xD, M);
+        order_step<2>(eo, gb, M);  order_step<3>(eo, gb, M);  order_step<5>(eo, gb, M);  order_step<7>(eo, gb, M);
+        order_step<11>(eo, gb, M); order_step<13>(eo, gb, M); order_step<17>(eo, gb, M); order_step<19>(eo, gb, M);
+        order_step<23>(eo, gb, M); order_step<29>(eo, gb, M); order_step<31>(eo, gb, M); order_step<37>(eo, gb, M);
+        order_step<41>(eo, gb, M); order_step<43>(eo, gb, M); order_step<47>(eo, gb, M); order_step<53>(eo, gb, M);
+        order_step<59>(eo, gb, M); order_step<61>(eo, gb, M);
+    }
     const u32 e = split_modulus(eo);
     const u64 xe = eo / e;
     const u64 s = mpow_call(bm, e, M);
@@ -268,59 +300,48 @@ __device__ __forceinline__ void fpow_multi(double (&a)[4], const double (&x)[4],
     for (int r = 0; r < R; ++r) a[r] = (a[r] < 0.0) ? a[r] + pd : a[r];
 }
 
-// At most two chains at a time: FP64 products have short enough latencies,
-// and four interleaved chains would not fit the kernel's 64 registers.
-__device__ __forceinline__ void fpow_lanes(u32 R, double (&a)[4], const double (&x)[4], u64 ex, double pd, double pinv)
-{
-    if (R == 1) {
-        fpow_multi<1>(a, x, ex, pd, pinv);
-        return;
-    }
-    fpow_multi<2>(a, x, ex, pd, pinv);
-    if (R > 2) {
-        double a2[4], x2[4] = {x[2], x[3], x[3], x[3]};
-        if (R == 3) fpow_multi<1>(a2, x2, ex, pd, pinv);
-        else fpow_multi<2>(a2, x2, ex, pd, pinv);
-        a[2] = a2[0];
-        a[3] = a2[1];
-    }
-}
-
-// z[r] = chi(k_i) = k_i^xD in Montgomery form for the lane's sequences
-// i = lane + 32r < K (1 elsewhere).  (Out of line, with the caller's state
+// z = chi(k_i) = k_i^xD in Montgomery form for the lane's sequences
+// i = lane + 32r < K, into zs[i].  (Out of line, with the caller's state
 // saved once per prime instead of spilled, it measured 3-6% slower.)
-struct Chi4 {
-    u64 z[4];
-};
-__device__ __forceinline__ Chi4 chi_of_ks(const JobDev *__restrict__ job, u32 lane, u32 K, const Mont M, u64 xD)
+// Below FP_BOUND the chains run on the FP64 pipe two at a time (four
+// interleaved chains would not fit the kernel's 64 registers), as a rolled
+// loop over pairs of rounds so that one copy of the chain code serves them.
+__device__ __forceinline__ void chi_of_ks(const JobDev *__restrict__ job, u32 lane, u32 K, const Mont M, u64 xD,
+                                          u64 *zs)
 {
     const u64 p = M.p;
     const u32 R = (K + 31) / 32;
-    Chi4 out;
     if (p < FP_BOUND) {
-        double x[4], zd[4];
+        const double pd = fp_exact(p), pinv = 1.0 / pd;
+#pragma unroll 1
+        for (u32 r0 = 0; r0 < R; r0 += 2) {
+            double x[4], zd[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const u32 i = lane + 32 * r;
-            const u64 kv = (i < K) ? job->k[i] : 1;
-            x[r] = fp_exact((kv < p) ? kv : kv % p);
+            for (u32 h = 0; h < 2; ++h) {
+                const u32 i = lane + 32 * (r0 + h);
+                const u64 kv = (i < K) ? job->k[i] : 1;
+                x[h] = fp_exact((kv < p) ? kv : kv % p);
+            }
+            if (r0 + 1 < R) fpow_multi<2>(zd, x, xD, pd, pinv);
+            else fpow_multi<1>(zd, x, xD, pd, pinv);
+#pragma unroll
+            for (u32 h = 0; h < 2; ++h)
+                if (r0 + h < R) zs[lane + 32 * (r0 + h)] = to_mont(fp_int(zd[h]), M);
         }
-        const double pd = (double)p;
-        fpow_lanes(R, zd, x, xD, pd, 1.0 / pd);
-#pragma unroll
-        for (int r = 0; r < 4; ++r) out.z[r] = to_mont(fp_int(zd[r]), M);
     } else {
-        u64 x[4];
+        u64 x[4], z[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const u32 i = lane + 32 * r;
             const u64 kv = (i < K) ? job->k[i] : 1;
             x[r] = to_mont((kv < p) ? kv : kv % p, M);
         }
-        if (p >> 62) mpow_lanes<false>(R, out.z, x, xD, M);
-        else mpow_lanes<true>(R, out.z, x, xD, M);
+        if (p >> 62) mpow_lanes<false>(R, z, x, xD, M);
+        else mpow_lanes<true>(R, z, x, xD, M);
+#pragma unroll
+        for (u32 r = 0; r < 4; ++r)
+            if (r < R) zs[lane + 32 * r] = z[r];
     }
-    return out;
 }
 
 // Class lookup: the e values h^(-r) (r < e <= SPLIT_MAX, all distinct and
@@ -421,12 +442,7 @@ __device__ __forceinline__ void setup_k_one(const JobDev *__restrict__ job, u32 
     // z = chi(k) = k^xD for the lane's sequences i = lane + 32r, r < R: one
     // exponent for the whole warp, R independent chains per lane
     const u32 R = (K + 31) / 32;
-    {
-        const Chi4 zc = chi_of_ks(job, lane, K, M, X.xD);
-#pragma unroll
-        for (u32 r = 0; r < 4; ++r)
-            if (r < R) zs[lane + 32 * r] = zc.z[r];
-    }
+    chi_of_ks(job, lane, K, M, X.xD, zs);
     __syncwarp();
     // pass 1: the class of every sequence; the kept ones' k mod p and class
     // offset go to the record (compacted), the target itself once Q' is known.

@@ -188,6 +188,26 @@ __device__ __forceinline__ u64 mhalf(u64 x, u64 n)
     return (x & 1) ? (x >> 1) + (n >> 1) + 1 : x >> 1;
 }
 
+// Selfridge's D for n (odd, not 1): the first of 5, -7, 9, -11, ... with
+// Jacobi (D/n) = -1.  Returns 0 when the search shows n composite (a common
+// factor, or n a square, which has no such D) and 1 when no D turned up
+// within 64 candidates; neither is a possible D.
+__device__ int selfridge_d(u64 n)
+{
+    int D = 5;
+    for (int tries = 0;; ++tries) {
+        if (tries == 64) return 1;
+        const u32 a = (u32)(D < 0 ? -D : D);
+        int j = jacobi32((u32)(n % a), a);                 // (n/a), then reciprocity
+        if ((a & 3) == 3 && (n & 3) == 3) j = -j;
+        if (D < 0 && (n & 3) == 3) j = -j;                 // (-1/n)
+        if (j == -1) return D;
+        if (j == 0) return 0;                              // gcd(a, n) > 1 with a < n
+        if (tries == 8 && is_square(n)) return 0;          // a square has no such D
+        D = (D > 0) ? -(D + 2) : (-D + 2);
+    }
+}
+
 // Strong Lucas probable-prime test with Selfridge's parameters: D is the first
 // of 5, -7, 9, -11, ... with Jacobi (D/n) = -1, P = 1, Q = (1 - D)/4; with
 // n + 1 = d * 2^s (d odd), n passes if U_d = 0 or V_(d*2^r) = 0 for some r < s.
@@ -204,18 +224,9 @@ __device__ __forceinline__ u64 mhalf(u64 x, u64 n)
 // caller then decides otherwise).  n is odd, above 65537^2 and below 2^64 - 1.
 __device__ int lucas_strong(u64 n, const Mont &M)
 {
-    int D = 5;
-    for (int tries = 0;; ++tries) {
-        if (tries == 64) return -1;
-        const u32 a = (u32)(D < 0 ? -D : D);
-        int j = jacobi32((u32)(n % a), a);                 // (n/a), then reciprocity
-        if ((a & 3) == 3 && (n & 3) == 3) j = -j;
-        if (D < 0 && (n & 3) == 3) j = -j;                 // (-1/n)
-        if (j == -1) break;
-        if (j == 0) return 0;                              // gcd(a, n) > 1 with a < n
-        if (tries == 8 && is_square(n)) return 0;          // a square has no such D
-        D = (D > 0) ? -(D + 2) : (-D + 2);
-    }
+    const int D = selfridge_d(n);
+    if (D == 0) return 0;
+    if (D == 1) return -1;
     const int Qi = (1 - D) / 4;
     const u64 Qm = to_mont(Qi >= 0 ? (u64)Qi : n - (u64)(-Qi), M);
     const int s = __ffsll((long long)(n + 1)) - 1;
@@ -242,6 +253,51 @@ __device__ int lucas_strong(u64 n, const Mont &M)
         }
     }
     return 0;
+}
+
+// lucas_strong for n < 2^51 on the FP64 pipe: the same ladder on plain
+// residues held exactly in doubles, products by fp_mul (1/n correctly
+// rounded), sums and differences exact in doubles with one correction each.
+__device__ int lucas_strong_fp(u64 n)
+{
+    const int D = selfridge_d(n);
+    if (D == 0) return 0;
+    if (D == 1) return -1;
+    const double nd = fp_exact(n), ninv = 1.0 / nd;
+    auto add = [&](double a, double b) { const double t = a + b; return (t >= nd) ? t - nd : t; };
+    auto sub = [&](double a, double b) { const double t = a - b; return (t < 0.0) ? t + nd : t; };
+    const int Qi = (1 - D) / 4;
+    const double Qd = fp_exact(Qi >= 0 ? (u64)Qi : n - (u64)(-Qi));
+    const int s = __ffsll((long long)(n + 1)) - 1;
+    const u64 d = (n + 1) >> s;
+    // k = 1: V_1 = P = 1, V_2 = P^2 - 2Q
+    double Vk = 1.0, Vk1 = sub(1.0, add(Qd, Qd)), Qk = Qd;
+    for (int bit = 62 - __clzll(d); bit >= 0; --bit) {
+        const bool one = (d >> bit) & 1;
+        const double t = fp_mul(Qk, one ? Qd : 1.0, nd, ninv);          // Q^(k+b)
+        const double mid = sub(fp_mul(Vk, Vk1, nd, ninv), Qk);          // V_(2k+1)
+        const double vs = one ? Vk1 : Vk;
+        const double sq = sub(fp_mul(vs, vs, nd, ninv), add(t, t));     // V_(2(k+b))
+        Qk = fp_mul(Qk, t, nd, ninv);
+        Vk = one ? mid : sq;
+        Vk1 = one ? sq : mid;
+    }
+    if (add(Vk1, Vk1) == Vk) return 1;                     // U_d = 0
+    double V = Vk;
+    for (int r = 0; r < s; ++r) {
+        if (V == 0.0) return 1;
+        if (r + 1 < s) {
+            V = sub(fp_mul(V, V, nd, ninv), add(Qk, Qk));
+            Qk = fp_mul(Qk, Qk, nd, ninv);
+        }
+    }
+    return 0;
+}
+
+// The strong Lucas test on the pipe that suits n.
+__device__ __forceinline__ int lucas_test(u64 n)
+{
+    return (n < FP_BOUND) ? lucas_strong_fp(n) : lucas_strong(n, mont_init(n));
 }
 
 // Strong probable prime to base 2: 2^d by squarings with a doubling (an
@@ -381,7 +437,7 @@ __global__ void __launch_bounds__(256) k_mr_lucas(const u64 *__restrict__ mid, c
         bool pr = false;
         if (idx < n) {
             v = mid[idx];
-            const int l = lucas_strong(v, mont_init(v));
+            const int l = lucas_test(v);
             pr = (l >= 0) ? (l == 1) : is_prime_mr(v);
         }
         warp_push(pr, v, primes, prime_cap, prime_ctr, err, ERR_PRIME_OVERFLOW);
@@ -444,7 +500,7 @@ __global__ void __launch_bounds__(256) k_mr_batch_lucas(const u64 *__restrict__ 
     const u32 n = min(*mid_ctr, mid_cap);
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const u64 v = mid[i];
-        const int l = lucas_strong(v, mont_init(v));
+        const int l = lucas_test(v);
         if (!((l >= 0) ? (l == 1) : is_prime_mr(v))) continue;
         const u32 r = mid_r[i];
         const u32 pos = atomicAdd(&ctrs[r * BR_CTRS + 1], 1u);
