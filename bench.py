@@ -35,11 +35,11 @@ WORKLOAD = ("config2 plain form: 100 seqs k*2^n+-1 (50 +1, 50 -1), k odd U[3,2^3
             "kept w.p. 0.03, p windows from 2^50")
 P_START = 1 << 50
 # DRAM bytes (read + write) per prime of the BSGS kernel, from one ncu capture
-# of a 2^20-wide window at 2^50 at the tuned Q = 8192 (69.18 MB for 30 203
-# primes, FP64 steps): the 2272-byte prime record plus claims.  Traffic grows
-# in proportion to primes, so the per-launch figure is this times the primes
-# one launch processes.
-BSGS_DRAM_BYTES_PER_PRIME = 2290.5
+# of a 2^20-wide window at 2^50 at the tuned Q = 8192 (69.36 MB for 30 203
+# primes, FP64 steps and start values): the 2272-byte prime record plus
+# claims.  Traffic grows in proportion to primes, so the per-launch figure is
+# this times the primes one launch processes.
+BSGS_DRAM_BYTES_PER_PRIME = 2296.4
 
 
 def reference_params(nmin, nmax):
@@ -96,7 +96,7 @@ def parse():
     ap.add_argument("--serve-rates", default="", help="extra arrival rates (units/s, comma-separated) to serve")
     ap.add_argument("--form", default="",
                     help="run only this form (config1, batched, batched_config2, batched_config4, served, "
-                         "served_stated) and print its result, for profiling it on its own")
+                         "served_stated, served_stated_low) and print its result, for profiling it on its own")
     ap.add_argument("--job", default="config2",
                     help="job of the timed steps: config2 (the benchmark), config1, config4 or config3:<index>; "
                          "the others are for profiling single kernels on those shapes")
@@ -405,6 +405,10 @@ def forms_of(torch, rs, W, peak, value, job, names):
             rs, W, serve, peak, seed=6, nunits=5, width_log2=(30, 31), rho=0.5, primes_per_s=value,
             label="config5 units at the lower end of their stated widths: 5 units of 2^U{30..31} over 16 files, "
                   "starts log-uniform in [2^44, 2^62], Poisson arrivals at the rate that loads the GPU to 0.5"),
+        "served_stated_low": lambda: measure_served(
+            rs, W, serve, peak, seed=6, nunits=5, width_log2=(30, 31), rho=0.3, primes_per_s=value,
+            label="config5 units at the lower end of their stated widths: 5 units of 2^U{30..31} over 16 files, "
+                  "starts log-uniform in [2^44, 2^62], Poisson arrivals at the rate that loads the GPU to 0.3"),
     }
     return {n: makers[n]() for n in names}
 
@@ -577,7 +581,8 @@ def main():
     forms = None
     if rank == 0 and world == 1 and not args.no_forms:
         forms = forms_of(torch, rs, W, peak, value, W.config2(args.seed),
-                         ["config1", "batched", "batched_config2", "batched_config4", "served", "served_stated"])
+                         ["config1", "batched", "batched_config2", "batched_config4", "served", "served_stated",
+                          "served_stated_low"])
         rates = [float(x) for x in args.serve_rates.split(",") if x] if args.serve_rates else []
         if rates:
             from rssieve_b200 import serve

@@ -555,48 +555,62 @@ __device__ __forceinline__ void setup_tabs_one(const JobDev *__restrict__ job, u
     for (u32 c = cp >> 1; c > 1; c >>= 1) u2 = mmul(u2, u2, p, q);
     const u64 u = mmul(u2, u2, p, q);
     u64 *tb = tabs + (size_t)t * TABS;
-    // four power tables, two chains at a time.  Below FP_BOUND the BSGS kernel
-    // forms its start values with FP64 products of plain residues, x*y mod p
-    // instead of x*y/R: there Z2, s^(cp/2) and S^(Lc/2) are stored plain, so
-    // baby and giant values alike carry R^2 instead of R; and the tables' own
-    // chains run on the FP64 pipe with plain multipliers (an R-form start
-    // times plain powers stays in R-form).
+    // four power tables, two chains at a time, each only as long as the BSGS
+    // kernel reads it: A[t % 32] and B[t / 32] for its threads t < tpb, Z1[g % 32]
+    // and Z2[g / 32] for the giant chunks g < G (the rest of the record's table
+    // space is left as it is).  Below FP_BOUND the BSGS kernel forms its start
+    // values with FP64 products of plain residues, x*y mod p instead of x*y/R:
+    // there Z2, s^(cp/2) and S^(Lc/2) are stored plain, so baby and giant values
+    // alike carry R^2 instead of R; and the tables' own chains run on the FP64
+    // pipe with plain multipliers (an R-form start times plain powers stays in
+    // R-form).  z^32 is needed only when G > 32, and then the Z1 chain has run
+    // all 32 steps.
+    const u32 nb = gm.tpb >> 5, nz1 = min(G, 32u), nz2 = (G + 31) >> 5;
     const bool fp = (p < FP_BOUND);
     if (fp) {
         const double pd = (double)p, pinv = 1.0 / pd;
         const double up = fp_exact(from_mont(u, M)), zp = fp_exact(from_mont(z, M));
         double a = fp_exact(M.one), b = a;
-        for (int l = 0; l < 32; ++l) {
+        for (u32 l = 0; l < 32; ++l) {
             tb[l] = fp_int(a);
-            tb[64 + l] = fp_int(b);
             a = fp_mul(a, up, pd, pinv);
-            b = fp_mul(b, zp, pd, pinv);
+            if (l < nz1) {
+                tb[64 + l] = fp_int(b);
+                b = fp_mul(b, zp, pd, pinv);
+            }
         }
-        const double u32p = fp_exact(from_mont(fp_int(a), M)), z32 = fp_exact(from_mont(fp_int(b), M));   // plain u^32, z^32
+        const double u32p = fp_exact(from_mont(fp_int(a), M));                  // plain u^32
+        const double z32 = (nz2 > 1) ? fp_exact(from_mont(fp_int(b), M)) : 0.0;  // plain z^32
         a = fp_exact(M.one);
         b = 1.0;
-        for (int l = 0; l < 32; ++l) {
+        for (u32 l = 0; l < nb; ++l) {
             tb[32 + l] = fp_int(a);
-            tb[96 + l] = fp_int(b);
             a = fp_mul(a, u32p, pd, pinv);
-            b = fp_mul(b, z32, pd, pinv);
+            if (l < nz2) {
+                tb[96 + l] = fp_int(b);
+                b = fp_mul(b, z32, pd, pinv);
+            }
         }
     } else {
         u64 a = M.one, b = M.one;
-        for (int l = 0; l < 32; ++l) {
+        for (u32 l = 0; l < 32; ++l) {
             tb[l] = a;
-            tb[64 + l] = b;
             a = mmul(a, u, p, q);
-            b = mmul(b, z, p, q);
+            if (l < nz1) {
+                tb[64 + l] = b;
+                b = mmul(b, z, p, q);
+            }
         }
-        const u64 u32p = a, z32 = b;                       // u^32, z^32
+        const u64 u32p = a, z32 = b;                       // u^32, and z^32 when G > 32
         a = M.one;
         b = M.one;
-        for (int l = 0; l < 32; ++l) {
+        for (u32 l = 0; l < nb; ++l) {
             tb[32 + l] = a;
-            tb[96 + l] = b;
             a = mmul(a, u32p, p, q);
-            b = mmul(b, z32, p, q);
+            if (l < nz2) {
+                tb[96 + l] = b;
+                b = mmul(b, z32, p, q);
+            }
         }
     }
     PrimeHdr &h = hdr[t];
