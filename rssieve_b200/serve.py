@@ -39,6 +39,25 @@ class Unit:
     bitmap: np.ndarray = field(default=None, repr=False)
 
 
+# Relative cost of one prime by the kind of step its p takes in the library:
+# FP64 products below 2^51, Shoup products below 2^63, Montgomery products
+# above.  Measured on a B200 with config-2-style units served one at a time:
+# 4.0e11 model cost units/s below 2^51 against 2.8-3.0e11 for units between
+# 2^52 and 2^61, i.e. a prime there costs 1.38 times as much.  Above 2^63 the
+# steps and the set-up's chains are full Montgomery products; the factor there
+# is the config-4 job's step rate against config 2's (253 against 427 G
+# steps/s in the BSGS kernel), an estimate for whole units.
+STEP_COST = ((1 << 51, 1.0), (1 << 63, 1.38), (1 << 64, 1.7))
+
+
+def step_factor(p0):
+    """Cost of a prime at p0 relative to one below 2^51 (STEP_COST)."""
+    for bound, f in STEP_COST:
+        if p0 < bound:
+            return f
+    return STEP_COST[-1][1]
+
+
 def cost_per_prime(q, kcount, L):
     """Model cost of one prime in baby-step units for Q baby steps (the library's
     geometry model: Q baby steps plus the giant steps of the surviving targets,
@@ -53,7 +72,7 @@ class Server:
 
     Each round, units are put in priority order (earliest deadline first by
     default, or least remaining work first; work is primes left times the model
-    cost of one prime for the unit's file) and given primes to cover from a
+    cost of one prime for the unit's file and step kind) and given primes to cover from a
     round budget of ROUND_S seconds of the measured throughput, so that a short
     unit arriving while long ones run finishes within a round or two.  A unit
     spreads over at most MAX_SPLIT range slots, enough to take a whole round's
@@ -99,9 +118,13 @@ class Server:
     def close(self):
         self.batch.close()
 
+    def _unit_cost(self, u):
+        """Model cost of one prime of unit u: its file's cost at the unit's step kind."""
+        return self.cost[self.templates[u.file]] * step_factor(u.p0)
+
     def _work(self, u, width):
         """Model cost of sieving `width` of unit u's p-range."""
-        return width / math.log(max(u.p0, 3)) * self.cost[self.templates[u.file]]
+        return width / math.log(max(u.p0, 3)) * self._unit_cost(u)
 
     def _budgets(self, active, remaining, given):
         """Primes per unit for the next round, in priority order, from a budget of
@@ -132,7 +155,7 @@ class Server:
             if budget is None:                    # first round: full windows
                 n = 1 << 40
             else:
-                c = self.cost[self.templates[active[slot].file]]
+                c = self._unit_cost(active[slot])
                 give = min(left(slot), budget)
                 budget -= give
                 n = int(math.ceil(give / c)) if give > 0 else 0
@@ -189,7 +212,7 @@ class Server:
             done, primes, rem = self.batch.poll()
             dt = clock() - r0
             self.busy_s += dt
-            work = sum(float(primes[s] - primes_seen[s]) * self.cost[self.templates[active[s].file]] for s in active)
+            work = sum(float(primes[s] - primes_seen[s]) * self._unit_cost(active[s]) for s in active)
             if trace is not None:
                 trace.append({"t": r0 - t0, "dt": dt, "rate": self.rate, "work": work, "queue": len(queue),
                               "free": self.batch.free_slots(),

@@ -191,6 +191,26 @@ def test_deadline_order_lets_a_waiting_long_unit_overtake(monkeypatch):
         assert got[other] == 0
 
 
+def test_deadlines_price_primes_by_step_kind(monkeypatch):
+    """Two units of one file arrive together, one below 2^51 (FP64 steps) and one
+    above (integer steps, 1.38 times the cost per prime).  The one below has more
+    primes, so a model without the step kind estimated it longer alone and gave
+    the round to the other; priced by step kind it is the shorter one and has
+    the earlier deadline."""
+    clock = Clock()
+    lo = serve.Unit(0, 0, 1 << 45, (1 << 45) + (1 << 28), 0.0)
+    hi = serve.Unit(1, 0, 1 << 54, (1 << 54) + (1 << 28), 0.1)
+    assert serve.step_factor(lo.p0) == 1.0 and serve.step_factor(hi.p0) > 1.3
+    srv, b = _server(monkeypatch, clock, footprints=(100,))
+    cost = srv.cost[srv.templates[0]]
+    srv.rate = cost * 1e7
+    assert srv._work(lo, lo.p1 - lo.p0) < srv._work(hi, hi.p1 - hi.p0)
+    # without the step kind the unit below 2^51 has the larger work
+    assert (lo.p1 - lo.p0) / math.log(lo.p0) > (hi.p1 - hi.p0) / math.log(hi.p0)
+    got = _budget_order(srv, b, [lo, hi])
+    assert got[0] > 0 and got[1] == 0
+
+
 def test_policy_must_be_known(monkeypatch):
     clock = Clock()
     with pytest.raises(ValueError):
