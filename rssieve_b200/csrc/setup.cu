@@ -99,14 +99,20 @@ __device__ __forceinline__ void order_step_fp(u64 &eo, double g, double p, doubl
     while (eo % L == 0 && fpow_call(g, eo / L, p, pinv) == 1.0) eo /= L;
 }
 
-// Largest divisor of eo that is at most SPLIT_MAX.
+// Largest divisor of eo that is at most SPLIT_MAX (by 32-bit remainders when
+// eo fits in 32 bits, the usual case, and from the largest candidate down).
 __device__ __forceinline__ u32 split_modulus(u64 eo)
 {
-    u32 e = 1;
+    if (eo >> 32) {
+        for (u32 d = SPLIT_MAX; d > 1; --d)
+            if (eo % d == 0) return d;
+        return 1;
+    }
+    const u32 e32 = (u32)eo;
 #pragma unroll
     for (u32 d = SPLIT_MAX; d > 1; --d)
-        if (e == 1 && eo % d == 0) e = d;
-    return e;
+        if (e32 % d == 0) return d;
+    return 1;
 }
 
 // b^e as an integer when it is at most 16 (baby steps by additions), else 0.
@@ -170,10 +176,24 @@ __device__ __forceinline__ void setup_prime_one(const JobDev *__restrict__ job, 
     X.e = e;
     const bool chi_m1 = (xD & 1) != 0;                    // chi(-1) = (-1)^xD
     X.flags = ((chi_m1 && (eo & 1)) ? AUX_NEG_EO : 0u) | ((chi_m1 && (xe & 1)) ? AUX_NEG_XE : 0u);
-    // Q'_k = 2^(m+2-k), m = log2(Q/4): s^(Q'-1) by t <- t^2 * s from s^(2^m - 1)
-    {
+    // Q'_k = 2^(m+2-k), m = log2(Q/4): s^(Q'-1) by t <- t^2 * s from s^(2^m - 1).
+    // Below FP_BOUND the powers are FP64 products of plain residues, moved
+    // into Montgomery form (and R^2 form for wr0) at the end.
+    const int m = __ffs((int)(gm.q >> 2)) - 1;
+    if (p < FP_BOUND) {
+        const double pd = fp_exact(p), pinv = 1.0 / pd;
+        const double sd = fp_exact(from_mont(s, M));
+        const double bn = fpow_call(fp_exact(b % p), (u64)job->nmin, pd, pinv);
+        double tq = 1.0;
+        for (int i = 0; i < m; ++i) tq = fp_mul(fp_mul(tq, tq, pd, pinv), sd, pd, pinv);
+#pragma unroll
+        for (int k = NCP - 1; k >= 0; --k) {              // k = NCP-1: Q/4, then Q/2, Q
+            if (k != NCP - 1) tq = fp_mul(fp_mul(tq, tq, pd, pinv), sd, pd, pinv);
+            X.wr0[k] = mmul(to_mont(fp_int(fp_mul(bn, tq, pd, pinv)), M), M.r2, p, M.q);
+            X.S[k] = to_mont(fp_int(fp_mul(tq, sd, pd, pinv)), M);
+        }
+    } else {
         const u64 bn = mpow_call(bm, (u64)job->nmin, M);
-        const int m = __ffs((int)(gm.q >> 2)) - 1;
         u64 tq = M.one;
         for (int i = 0; i < m; ++i) tq = mmul(mmul(tq, tq, p, M.q), s, p, M.q);
 #pragma unroll
